@@ -1,0 +1,168 @@
+/*
+ * xnyz.h - C ABI of the B200-native XnYZip compress/decompress path.
+ *
+ * Every compute stage runs as a hand-written sm_100a CUDA kernel; host code only builds
+ * Huffman codebooks (they depend on libstdc++ container order, see below), writes the
+ * container header and calls libzstd.  Signatures use plain pointers and sizes only.
+ *
+ * Reference interfaces replaced (paths relative to the reference's source/ directory):
+ *   xnyz_compress    <- XnYZip::BlockCompressor<float>::compress        composer/block_compressor.hpp:35,39
+ *                       XnYZip::BlockCompressorRLE<float>::compress     composer/block_compressor_rle.hpp:34,38
+ *   xnyz_decompress  <- XnYZip::BlockDecompressor<float>::decompress    composer/block_decompressor.hpp:27,31
+ *                       XnYZip::BlockDecompressorRLE<float>::decompress composer/block_decompressor_rle.hpp:28,32
+ *   quantizer codes  <- XnYZip::QUANTIZER_TYPE {CUBE, TRUNCATED_OCTAHEDRON} composer/utils.hpp:55-59
+ *   stage entry points (xnyz_stage_*) <- shift_points preprocessor/shifting.hpp:11,
+ *       TruncatedOctahedronQuantizer/CubeQuantizer::quantize/recover quantizer/truncated_octahedron_quantizer.hpp, cube_quantizer.hpp,
+ *       mve::mortonToHilbert3/hilbertToMorton3 quantizer/hilbert-curves-cpp/hilbert.hpp:8-9,
+ *       radix_sort quantizer/block_quantizer.hpp:33.
+ *
+ * Errors are status codes; nothing throws across this boundary.  Calls on one context are
+ * serialised on that context's CUDA stream; contexts are independent.
+ */
+#ifndef XNYZ_H
+#define XNYZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum xnyz_status {
+    XNYZ_OK = 0,
+    XNYZ_ERR_INVALID_ARG = 1,  /* bad argument (null pointer, n == 0, unknown quantizer, ...) */
+    XNYZ_ERR_BAD_STREAM = 2,   /* malformed or truncated container / bit stream */
+    XNYZ_ERR_CUDA = 3,         /* a CUDA runtime call failed; see xnyz_last_error() */
+    XNYZ_ERR_OOM = 4,          /* device or host allocation failed */
+    XNYZ_ERR_TIMEOUT = 5,      /* a bounded device-side wait expired (kernel returned early) */
+    XNYZ_ERR_UNSUPPORTED = 6,  /* input outside the supported envelope (e.g. > 64 key bits) */
+    XNYZ_ERR_ZSTD = 7,         /* libzstd 1.5.7 missing, wrong version, or it reported an error */
+    XNYZ_ERR_NO_DEVICE = 8     /* no CUDA device / the library was not built for this device */
+} xnyz_status;
+
+/* Quantizer codes (values follow XnYZip::QUANTIZER_TYPE). */
+enum { XNYZ_QUANT_CUBE = 0, XNYZ_QUANT_TO = 1 };
+
+typedef struct xnyz_ctx xnyz_ctx;
+
+/* Per-call configuration, mirroring the reference constructors and CLI flags. */
+typedef struct xnyz_params {
+    int quantizer;        /* XNYZ_QUANT_CUBE or XNYZ_QUANT_TO ("cube" / "to") */
+    float l2_bound;       /* the L2 bound (CLI argv[3]) */
+    int hilbert;          /* 1 = Hilbert curve ("-h"), 0 = Morton / z-order ("-z") */
+    int rle;              /* 1 = "-rle" container, 0 = "-normal" */
+    int direct_threshold; /* direct SFC mode when max range < threshold (CLI default 1024; 0 forces block) */
+} xnyz_params;
+
+/* Statistics of the last compress call (what the reference prints on stdout). */
+typedef struct xnyz_compress_info {
+    uint64_t num_points;      /* input points */
+    uint64_t num_units;       /* unique cells (-rle) or points (-normal) */
+    uint64_t num_blocks;      /* 128^3 super-block runs (block mode) */
+    uint64_t num_patches;     /* PFor patches of the repos / SFC-delta stream */
+    uint64_t container_bytes; /* pre-zstd container size */
+    uint64_t output_bytes;    /* bytes returned (zstd frame, or container when zstd is off) */
+    int32_t range[3];         /* max lattice index per axis (container fields) */
+    int is_direct;            /* 1 = direct SFC mode, 0 = block mode */
+    int counts_exp_golomb;    /* 1 if the -rle count stream switched to exp-Golomb */
+    double max_l2_error;      /* max |p - recover(quantize(p))| (block_compressor_rle.hpp:53-67) */
+    double mse;               /* mean squared error of the same */
+    double gpu_ms;            /* device time of the call (CUDA events) */
+} xnyz_compress_info;
+
+/* ---- context ------------------------------------------------------------------------ */
+
+/* Creates a context on `device`.  `stream` (a cudaStream_t, may be NULL) is the stream all
+ * work of this context is issued on; NULL creates a private non-blocking stream. */
+xnyz_status xnyz_create(xnyz_ctx** ctx, int device, void* stream);
+xnyz_status xnyz_destroy(xnyz_ctx* ctx);
+/* Message of the last error on this thread (static storage, never NULL). */
+const char* xnyz_last_error(void);
+/* Library version string. */
+const char* xnyz_version(void);
+
+/* Path of libzstd 1.5.7 (loaded on first use; the environment variable XNYZ_ZSTD_LIBRARY
+ * overrides).  Returns XNYZ_ERR_ZSTD if it cannot be loaded or is not version 1.5.7. */
+xnyz_status xnyz_set_zstd_library(const char* path);
+
+/* Pinned host buffers (cudaHostAlloc) for fast host<->device copies. */
+xnyz_status xnyz_host_alloc(void** ptr, size_t bytes);
+xnyz_status xnyz_host_free(void* ptr);
+
+/* Releases the context's cached device workspace. */
+xnyz_status xnyz_trim(xnyz_ctx* ctx);
+
+/* ---- whole path ------------------------------------------------------------------------ */
+
+/* Compress n float32 xyz points (AoS, 12 bytes each).
+ *   xyz_is_device : 1 if `xyz` is a device pointer, 0 if host memory (copied in).
+ *   use_zstd      : 1 -> output is the zstd level-3 frame the reference returns
+ *                   (composer/utils.hpp:35-53); 0 -> the raw pre-zstd container.
+ *   out/out_len   : malloc'd host buffer with the result; release with xnyz_free().
+ *   sort_order    : optional host array of n uint64 receiving, for each position of the
+ *                   container's point order, the index of the input point (what
+ *                   compress() does to its argument, block_compressor.hpp:141-144); NULL to skip.
+ *   info          : optional statistics. */
+xnyz_status xnyz_compress(xnyz_ctx* ctx, const float* xyz, uint64_t n, int xyz_is_device, const xnyz_params* params,
+                          int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order,
+                          xnyz_compress_info* info);
+
+/* Compress into a device-resident container.  `xyz` is a device pointer; the container
+ * stays in the context's workspace and is described by (*dev_container, *container_len)
+ * until the next call on the context. */
+xnyz_status xnyz_compress_device(xnyz_ctx* ctx, const float* xyz, uint64_t n, const xnyz_params* params,
+                                 const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info);
+
+/* Decompress.  `in` is host memory holding a zstd frame (is_zstd = 1) or a raw container.
+ * quantizer / l2_bound / rle must be the values used to compress (the container does not
+ * record them, exactly as in the reference).  The result is written to a malloc'd host
+ * array of 3*n floats (*xyz, release with xnyz_free) in the container's point order. */
+xnyz_status xnyz_decompress(xnyz_ctx* ctx, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                            float l2_bound, int rle, float** xyz, uint64_t* n);
+
+/* Decompress a device-resident raw container into a device array owned by the context
+ * (valid until the next call).  Host code reads the few header fields it needs. */
+xnyz_status xnyz_decompress_device(xnyz_ctx* ctx, const uint8_t* dev_container, uint64_t len, int quantizer,
+                                   float l2_bound, int rle, const float** dev_xyz, uint64_t* n);
+
+void xnyz_free(void* p);
+
+/* ---- stage entry points (device pointers; used by the parity tests) ------------------ */
+
+/* shift_points + quantize: offset3 (host, 3 floats) and cells (device, 3*n int32). */
+xnyz_status xnyz_stage_quantize(xnyz_ctx* ctx, const float* dev_xyz, uint64_t n, int quantizer, float l2_bound,
+                                float* offset3, int32_t* dev_cells);
+/* quantizer->recover + unshift_points on device cells. */
+xnyz_status xnyz_stage_recover(xnyz_ctx* ctx, const int32_t* dev_cells, uint64_t n, int quantizer, float l2_bound,
+                               const float* offset3, float* dev_xyz);
+/* mortonToHilbert3 (inverse = 0) or hilbertToMorton3 (inverse = 1) on n device codes. */
+xnyz_status xnyz_stage_hilbert(xnyz_ctx* ctx, const uint64_t* dev_in, uint64_t n, unsigned iteration, int inverse,
+                               uint64_t* dev_out);
+/* Stable LSD radix sort of n uint64 keys over bits [0, key_bits) with an optional uint32
+ * payload; results replace the inputs. */
+xnyz_status xnyz_stage_sort(xnyz_ctx* ctx, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits);
+
+/* ---- host-side helpers (no GPU needed) ----------------------------------------------- */
+
+/* The table-driven Hilbert transform the kernels use, evaluated on the host
+ * (mortonToHilbert3 / hilbertToMorton3, quantizer/hilbert-curves-cpp/hilbert.cpp:412-464). */
+xnyz_status xnyz_host_hilbert(const uint64_t* in, uint64_t n, unsigned iteration, int inverse, uint64_t* out);
+
+/* Huffman / exp-Golomb codebook of one stream from per-symbol statistics, exactly as
+ * HuffmanEncoder<T>::build + get_meta produce it (encoder/huffman_encoder.hpp:33-147).
+ *   symtype      : 0 uint64_t, 1 uint8_t, 2 int
+ *   count_stream : 1 = the -rle count stream's build / measure / rebuild sequence
+ *                  (composer/block_compressor_rle.hpp:290-303)
+ *   symbols, counts, first_index : nsyms distinct symbols, their frequencies and the index
+ *                  of their first occurrence; total = number of symbols in the data
+ *   meta         : receives up to *meta_len bytes; *meta_len is set to the meta size */
+xnyz_status xnyz_host_codebook(int symtype, int count_stream, const uint64_t* symbols, const uint64_t* counts,
+                               const uint64_t* first_index, uint64_t nsyms, uint64_t total, uint8_t* meta,
+                               uint64_t* meta_len, uint64_t* encoded_bits, int* exp_golomb);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XNYZ_H */

@@ -1,0 +1,190 @@
+"""XnYZip compress/decompress path on B200 (sm_100a).
+
+Python mirror of the reference's composer interface (composer/block_compressor.hpp,
+composer/block_compressor_rle.hpp, composer/block_decompressor.hpp,
+composer/block_decompressor_rle.hpp, composer/utils.hpp) over the C ABI of libxnyz.so:
+
+    BlockCompressor(QUANTIZER_TYPE.TRUNCATED_OCTAHEDRON, 0.05).compress(points, curve_type)
+    BlockDecompressor(QUANTIZER_TYPE.TRUNCATED_OCTAHEDRON, 0.05).decompress(data)
+
+`points` is an (n, 3) float32 array (numpy on the host, or a CUDA torch tensor); the
+result of compress() is the zstd frame the reference returns, byte for byte.  Every compute
+stage runs in hand-written CUDA kernels; the module raises ImportError if the library is
+not built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _native as N
+from ._native import CompressInfo, Params, XnyzError
+
+__all__ = ["QUANTIZER_TYPE", "Context", "BlockCompressor", "BlockCompressorRLE", "BlockDecompressor",
+           "BlockDecompressorRLE", "XnyzError", "CompressInfo", "default_context"]
+
+
+class QUANTIZER_TYPE(enum.IntEnum):
+    """composer/utils.hpp:55-59."""
+    CUBE = 0
+    TRUNCATED_OCTAHEDRON = 1
+    ADAPTIVE = 2
+
+
+def _is_torch_cuda(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+class Context:
+    """One device, one CUDA stream, one cached workspace (an xnyz_ctx)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = C.c_void_p()
+        N.check(N.create(C.byref(h), device, C.c_void_p(stream) if stream else None))
+        self.handle = h
+        self.device = device
+        self.last_info = CompressInfo()
+
+    def close(self):
+        if self.handle:
+            N.destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- whole path -------------------------------------------------------------------
+    def compress(self, points, quantizer: int, l2: float, hilbert: bool, rle: bool, direct_threshold: int = 1024,
+                 use_zstd: bool = True, want_order: bool = False):
+        prm = Params(int(quantizer), float(l2), int(bool(hilbert)), int(bool(rle)), int(direct_threshold))
+        out = C.POINTER(C.c_uint8)()
+        ln = C.c_uint64()
+        info = CompressInfo()
+        if _is_torch_cuda(points):
+            pts = points.contiguous()
+            n = pts.numel() // 3
+            ptr, on_dev = C.c_void_p(pts.data_ptr()), 1
+        else:
+            pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            n = pts.shape[0]
+            ptr, on_dev = pts.ctypes.data_as(C.c_void_p), 0
+        order = np.zeros(max(n, 1), dtype=np.uint64) if want_order else None
+        N.check(N.compress(self.handle, ptr, n, on_dev, C.byref(prm), int(use_zstd), C.byref(out), C.byref(ln),
+                           order.ctypes.data_as(C.c_void_p) if want_order else None, C.byref(info)))
+        try:
+            data = C.string_at(out, ln.value)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+        self.last_info = info
+        return (data, order[:n]) if want_order else data
+
+    def decompress(self, data: bytes, quantizer: int, l2: float, rle: bool, is_zstd: bool = True) -> np.ndarray:
+        buf = np.frombuffer(data, dtype=np.uint8)
+        out = C.POINTER(C.c_float)()
+        n = C.c_uint64()
+        N.check(N.decompress(self.handle, buf.ctypes.data_as(C.c_void_p), len(data), int(is_zstd), int(quantizer),
+                             float(l2), int(bool(rle)), C.byref(out), C.byref(n)))
+        try:
+            arr = np.ctypeslib.as_array(out, shape=(3 * n.value,)).copy() if n.value else np.zeros(0, np.float32)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+        return arr.reshape(-1, 3)
+
+    def compress_device(self, dev_ptr: int, n: int, quantizer: int, l2: float, hilbert: bool, rle: bool,
+                        direct_threshold: int = 1024):
+        """Device points -> device container (pointer, length) owned by the context."""
+        prm = Params(int(quantizer), float(l2), int(bool(hilbert)), int(bool(rle)), int(direct_threshold))
+        p = C.c_void_p()
+        ln = C.c_uint64()
+        info = CompressInfo()
+        N.check(N.compress_device(self.handle, C.c_void_p(dev_ptr), n, C.byref(prm), C.byref(p), C.byref(ln),
+                                  C.byref(info)))
+        self.last_info = info
+        return p.value, ln.value
+
+    def decompress_device(self, dev_ptr: int, length: int, quantizer: int, l2: float, rle: bool):
+        """Device container -> (device pointer to 3*n floats owned by the context, n)."""
+        p = C.c_void_p()
+        n = C.c_uint64()
+        N.check(N.decompress_device(self.handle, C.c_void_p(dev_ptr), length, int(quantizer), float(l2),
+                                    int(bool(rle)), C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+
+_default: Context | None = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+class _CompressorBase:
+    _rle = False
+
+    def __init__(self, quantizer_type: QUANTIZER_TYPE, l2_bound: float, is_debugging: bool = False,
+                 direct_threshold: int = 1024, context: Context | None = None):
+        if QUANTIZER_TYPE(quantizer_type) == QUANTIZER_TYPE.ADAPTIVE:
+            raise XnyzError(6, "the adaptive quantizer is not on the CLI path (main.cpp handles cube and to)")
+        self.quantizer = int(quantizer_type)
+        self.l2_bound = float(np.float32(l2_bound))
+        self.direct_threshold = int(direct_threshold)
+        self.ctx = context
+
+    def compress(self, points, curve_type: bool) -> bytes:
+        """Returns the zstd frame.  For -normal, reorders a numpy `points` array in place into
+        the container's point order, as the reference does with its argument
+        (block_compressor.hpp:141-144, 105-108)."""
+        ctx = self.ctx or default_context()
+        inplace = (not self._rle) and isinstance(points, np.ndarray)
+        res = ctx.compress(points, self.quantizer, self.l2_bound, bool(curve_type), self._rle, self.direct_threshold,
+                           use_zstd=True, want_order=inplace)
+        if inplace:
+            data, order = res
+            view = points.reshape(-1, 3)
+            view[:] = view[order.astype(np.int64)]
+            return data
+        return res
+
+
+class BlockCompressor(_CompressorBase):
+    """composer/block_compressor.hpp:31-39 (-normal container)."""
+    _rle = False
+
+
+class BlockCompressorRLE(_CompressorBase):
+    """composer/block_compressor_rle.hpp:30-38 (-rle container)."""
+    _rle = True
+
+
+class _DecompressorBase:
+    _rle = False
+
+    def __init__(self, quantizer_type: QUANTIZER_TYPE, l2_bound: float, is_debugging: bool = False,
+                 context: Context | None = None):
+        if QUANTIZER_TYPE(quantizer_type) == QUANTIZER_TYPE.ADAPTIVE:
+            raise XnyzError(6, "the adaptive quantizer is not on the CLI path")
+        self.quantizer = int(quantizer_type)
+        self.l2_bound = float(np.float32(l2_bound))
+        self.ctx = context
+
+    def decompress(self, compressed_data: bytes) -> np.ndarray:
+        ctx = self.ctx or default_context()
+        return ctx.decompress(compressed_data, self.quantizer, self.l2_bound, self._rle, is_zstd=True)
+
+
+class BlockDecompressor(_DecompressorBase):
+    """composer/block_decompressor.hpp:25-31."""
+    _rle = False
+
+
+class BlockDecompressorRLE(_DecompressorBase):
+    """composer/block_decompressor_rle.hpp:26-32."""
+    _rle = True

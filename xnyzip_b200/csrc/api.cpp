@@ -1,0 +1,1527 @@
+// C ABI and host orchestration of the B200 XnYZip path (declared in include/xnyz.h).
+//
+// Compress (BlockCompressor{,RLE}<float>::compress, composer/block_compressor.hpp:39-222,
+// composer/block_compressor_rle.hpp:38-321), every stage on the GPU:
+//   bbox -> quantize + ranges -> [host: mode, key layout] -> keys (+ digit histograms)
+//   -> LSD radix sort -> units (dedup, LCP deltas, PFor, histograms) -> count / block stats
+//   -> [host: Huffman codebooks from histograms, Golomb-Rice k, bit widths]
+//   -> bit-pack / Golomb-Rice / Huffman / exp-Golomb encoders -> container -> zstd (host).
+// Decompress (BlockDecompressor{,RLE}<float>::decompress): zstd (host) -> header (host)
+//   -> bit-unpack + prefix sums -> parallel Golomb-Rice / Huffman / exp-Golomb decoding
+//   -> fused LCP recovery, PFor decode, expansion, recover and unshift.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/xnyz.h"
+#include "host/codebook.h"
+#include "host/hilbert_tables.h"
+#include "host/zstd_dl.h"
+#include "kernels.h"
+
+using namespace xnyz;
+using namespace xnyz::dev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+xnyz_status fail(xnyz_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+#define CUDA_TRY(expr)                                                                               \
+    do {                                                                                             \
+        cudaError_t e_ = (expr);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? XNYZ_ERR_OOM : XNYZ_ERR_CUDA,              \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                         \
+    } while (0)
+
+#define TRY(expr)                          \
+    do {                                   \
+        xnyz_status s_ = (expr);           \
+        if (s_ != XNYZ_OK) return s_;      \
+    } while (0)
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+inline uint64_t cdiv(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+inline int bitlen(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
+
+// Fixed-size device state of a context (counters, histograms, code tables, tables).
+struct Small {
+    PointStats stats;
+    unsigned long long counters[8];
+    unsigned long long hist_rep[256];
+    uint32_t first_rep[256];
+    unsigned long long hist_quad[256];
+    uint32_t first_quad[256];
+    unsigned long long cnt_hist[kCountDense];
+    uint32_t cnt_first[kCountDense];
+    uint32_t over_n;
+    uint32_t err;
+    uint32_t fallback[8];
+    uint32_t maxrun[8];
+    unsigned long long max2[2];
+    unsigned long long totals[8];
+    unsigned long long codewords[8];
+    unsigned long long count_total;
+    uint32_t tile_counters[64];
+    uint32_t sort_hist[8 * 256];
+    ByteCodes codes[2];
+    uint8_t hil_fwd[256];
+    uint8_t hil_inv[256];
+    float offset_in[4];
+};
+
+// A growable device arena, carved per call.
+struct Arena {
+    char* base = nullptr;
+    size_t cap = 0;
+};
+
+struct Plan {
+    size_t total = 0;
+    size_t add(size_t bytes) {
+        const size_t o = align_up(total);
+        total = o + align_up(bytes ? bytes : 1);
+        return o;
+    }
+};
+
+}  // namespace
+
+struct xnyz_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Small* d_small = nullptr;
+    Small* h_small = nullptr;  // pinned mirror
+    Arena arena;
+    unsigned long long* sort_status = nullptr;
+    size_t sort_status_cap = 0;  // entries
+    uint32_t sort_epoch = 0;
+    uint8_t* h_stage = nullptr;  // pinned staging for containers
+    size_t h_stage_cap = 0;
+    uint8_t* d_container = nullptr;  // device container returned by xnyz_compress_device
+    size_t d_container_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+xnyz_status ensure_arena(xnyz_ctx* c, size_t bytes) {
+    if (c->arena.cap >= bytes) return XNYZ_OK;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->arena.base) cudaFree(c->arena.base);
+    c->arena.base = nullptr;
+    c->arena.cap = 0;
+    const size_t want = align_up(bytes + bytes / 8, 1 << 20);
+    CUDA_TRY(cudaMalloc(&c->arena.base, want));
+    c->arena.cap = want;
+    return XNYZ_OK;
+}
+
+xnyz_status ensure_host_stage(xnyz_ctx* c, size_t bytes) {
+    if (c->h_stage_cap >= bytes) return XNYZ_OK;
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    const size_t want = align_up(bytes + bytes / 8, 1 << 20);
+    CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&c->h_stage), want, cudaHostAllocDefault));
+    c->h_stage_cap = want;
+    return XNYZ_OK;
+}
+
+template <typename T>
+T* at(xnyz_ctx* c, size_t off) {
+    return reinterpret_cast<T*>(c->arena.base + off);
+}
+
+#define SMALL_FIELD(c, f) (&(c)->d_small->f)
+
+xnyz_status memset_small(xnyz_ctx* c, size_t off, size_t bytes, int v) {
+    CUDA_TRY(cudaMemsetAsync(reinterpret_cast<char*>(c->d_small) + off, v, bytes, c->stream));
+    return XNYZ_OK;
+}
+
+xnyz_status fetch_small(xnyz_ctx* c, size_t off, size_t bytes) {
+    CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c->h_small) + off, reinterpret_cast<char*>(c->d_small) + off,
+                             bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return XNYZ_OK;
+}
+
+xnyz_status check_device_errors(xnyz_ctx* c) {
+    TRY(fetch_small(c, offsetof(Small, err), sizeof(uint32_t)));
+    const uint32_t e = c->h_small->err;
+    if (e & 1u) return fail(XNYZ_ERR_TIMEOUT, "a bounded device wait expired");
+    if (e & 2u) return fail(XNYZ_ERR_BAD_STREAM, "malformed bit stream");
+    if (e & 4u) return fail(XNYZ_ERR_BAD_STREAM, "stream content exceeds its declared sizes");
+    return XNYZ_OK;
+}
+
+QuantParams make_quant(int quantizer, float l2) {
+    QuantParams q;
+    q.quantizer = quantizer;
+    const double k = quantizer == 1 ? 5.0 : 3.0;
+    // 2 * l2 in float, divided by sqrt(k) in double, stored as float (the reference's
+    // `pt / (2 * TRUNC_OCT_SCALE_ / sqrt(k))` with Eigen's scalar conversion).
+    q.div = static_cast<float>(static_cast<double>(2.0f * l2) / std::sqrt(k));
+    q.s = l2;
+    q.rdiv = static_cast<float>(std::sqrt(k));
+    return q;
+}
+
+uint64_t spread3_host(uint32_t v) {
+    uint64_t r = 0;
+    for (int b = 0; b < 21; ++b) r |= static_cast<uint64_t>((v >> b) & 1u) << (3 * b);
+    return r;
+}
+
+// ---------------------------------------------------------------- sort ------------------
+struct SortBufs {
+    unsigned long long* keys[2];
+    uint32_t* vals[2];
+};
+
+// Sorts keys (and payload) over `passes` 8-bit digits whose histograms are in hist (already
+// filled).  Returns the index of the buffer holding the result.
+xnyz_status radix_sort(xnyz_ctx* c, SortBufs& b, uint64_t n, int passes, uint32_t* d_hist, int& result) {
+    result = 0;
+    if (passes == 0 || n <= 1) return XNYZ_OK;
+    const uint64_t tiles = cdiv(n, kSortTile);
+    const size_t need = tiles * 256;
+    if (c->sort_status_cap < need) {
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->sort_status) cudaFree(c->sort_status);
+        c->sort_status = nullptr;
+        const size_t want = need + need / 4 + 4096;
+        CUDA_TRY(cudaMalloc(&c->sort_status, want * sizeof(unsigned long long)));
+        CUDA_TRY(cudaMemsetAsync(c->sort_status, 0, want * sizeof(unsigned long long), c->stream));
+        c->sort_status_cap = want;
+        c->sort_epoch = 0;
+    }
+    if (c->sort_epoch + passes >= 16383) {
+        CUDA_TRY(cudaMemsetAsync(c->sort_status, 0, c->sort_status_cap * sizeof(unsigned long long), c->stream));
+        c->sort_epoch = 0;
+    }
+    launch_sort_offsets(d_hist, passes, c->stream);
+    TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 8, 0));
+    int cur = 0;
+    for (int p = 0; p < passes; ++p) {
+        const uint32_t epoch = ++c->sort_epoch;
+        launch_sort_pass(b.keys[cur], b.keys[cur ^ 1], b.vals[cur], b.vals[cur ^ 1], n, 8 * p, d_hist + 256 * p,
+                         c->sort_status, epoch, SMALL_FIELD(c, tile_counters[p]), SMALL_FIELD(c, err), c->stream);
+        cur ^= 1;
+    }
+    CUDA_TRY(cudaGetLastError());
+    result = cur;
+    return XNYZ_OK;
+}
+
+// ---------------------------------------------------------------- container --------------
+struct Hole {
+    const void* dsrc;  // device source
+    size_t off;        // offset in the container
+    size_t bytes;
+};
+
+struct Container {
+    std::vector<uint8_t> skel;  // host bytes (holes zero)
+    std::vector<Hole> holes;
+    template <typename V>
+    void pod(V v) {
+        const uint8_t* p = reinterpret_cast<const uint8_t*>(&v);
+        skel.insert(skel.end(), p, p + sizeof(V));
+    }
+    // [u64 data_len][u64 meta_len][meta][data]  (block_compressor.hpp:152-155)
+    void stream(const std::vector<uint8_t>& meta, const void* ddata, size_t data_bytes) {
+        pod<uint64_t>(data_bytes);
+        pod<uint64_t>(meta.size());
+        skel.insert(skel.end(), meta.begin(), meta.end());
+        if (data_bytes) holes.push_back(Hole{ddata, skel.size(), data_bytes});
+        skel.resize(skel.size() + data_bytes, 0);
+    }
+};
+
+std::vector<uint8_t> le5(uint32_t n, uint8_t b) {
+    return {static_cast<uint8_t>(n), static_cast<uint8_t>(n >> 8), static_cast<uint8_t>(n >> 16),
+            static_cast<uint8_t>(n >> 24), b};
+}
+
+struct CompressOut {
+    Container cont;
+    xnyz_compress_info info{};
+    uint32_t* d_order = nullptr;  // -normal: input index per container position
+};
+
+// One chained-scan channel set in the arena.
+struct LB {
+    size_t flag, agg, inc;
+    uint64_t tiles;
+};
+LB plan_lb(Plan& pl, uint64_t tiles, int channels, int agg_words_per_tile = 1, int inc_words_per_tile = 1) {
+    LB l;
+    l.tiles = tiles;
+    l.flag = pl.add(sizeof(uint32_t) * tiles * channels);
+    l.agg = pl.add(sizeof(unsigned long long) * tiles * channels * agg_words_per_tile);
+    l.inc = pl.add(sizeof(unsigned long long) * tiles * channels * inc_words_per_tile);
+    return l;
+}
+LookBackState lb_state(xnyz_ctx* c, const LB& l) {
+    return LookBackState{at<uint32_t>(c, l.flag), at<unsigned long long>(c, l.agg), at<unsigned long long>(c, l.inc)};
+}
+xnyz_status lb_clear(xnyz_ctx* c, const LB& l, int channels) {
+    CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, l.flag), 0, sizeof(uint32_t) * l.tiles * channels, c->stream));
+    return XNYZ_OK;
+}
+
+// Arena layout of the compress path up to the encoder outputs (depends on n only).
+struct CPlan {
+    uint64_t tiles;
+    size_t o_k0, o_k1, o_v0, o_v1, o_rep, o_quad, o_patch, o_blkid, o_blkunit, o_unitpos, o_counts, o_over_v,
+        o_over_u, o_dblk, o_dcnt;
+    LB lb_units, lb_enc;
+    size_t total;
+};
+CPlan make_cplan(uint64_t n, bool want_order, size_t reserved) {
+    CPlan c{};
+    c.tiles = cdiv(n, kSortTile);
+    Plan pl;
+    pl.total = reserved;
+    c.o_k0 = pl.add(8 * n);
+    c.o_k1 = pl.add(8 * n);
+    c.o_v0 = want_order ? pl.add(4 * n) : 0;
+    c.o_v1 = want_order ? pl.add(4 * n) : 0;
+    c.o_rep = pl.add(n);
+    c.o_quad = pl.add(n);
+    c.o_patch = pl.add(8 * n);
+    c.o_blkid = pl.add(8 * n);
+    c.o_blkunit = pl.add(4 * n);
+    c.o_unitpos = pl.add(4 * n + 4);
+    c.o_counts = pl.add(4 * n);
+    c.o_over_v = pl.add(4 * n);
+    c.o_over_u = pl.add(4 * n);
+    c.o_dblk = pl.add(8 * n);
+    c.o_dcnt = pl.add(8 * n);
+    c.lb_units = plan_lb(pl, c.tiles, 3);
+    c.lb_enc = plan_lb(pl, c.tiles, 4);
+    c.total = pl.total;
+    return c;
+}
+// Typical encoder output space (grown on demand when a stream is larger).
+size_t encoder_reserve(uint64_t n) { return 4 * n + (8u << 20); }
+
+xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& prm, bool want_order,
+                          size_t arena_reserved, CompressOut& R) {
+    if (prm.quantizer != XNYZ_QUANT_CUBE && prm.quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    if (!(prm.l2_bound > 0.0f) || !std::isfinite(prm.l2_bound))
+        return fail(XNYZ_ERR_INVALID_ARG, "l2_bound must be a positive finite float");
+    if (n == 0) return fail(XNYZ_ERR_INVALID_ARG, "no points (the reference leaves the offset undefined for n = 0)");
+    if (n >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 points");
+    const bool rle = prm.rle != 0, hil = prm.hilbert != 0;
+    const QuantParams q = make_quant(prm.quantizer, prm.l2_bound);
+    cudaStream_t st = c->stream;
+
+    // ---- 1. bounding box + quantization sweep ----
+    {
+        PointStats init{};
+        for (int a = 0; a < 3; ++a) {
+            init.minkey[a] = ~0ull;
+            init.max_cell[a] = 0;
+            init.min_cell[a] = INT32_MAX;
+        }
+        c->h_small->stats = init;
+        c->h_small->err = 0;
+        CUDA_TRY(cudaMemcpyAsync(&c->d_small->stats, &c->h_small->stats, sizeof(PointStats), cudaMemcpyHostToDevice, st));
+        TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
+    }
+    launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
+    launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, stats), sizeof(PointStats)));
+    const PointStats S = c->h_small->stats;
+    if (S.nonfinite) return fail(XNYZ_ERR_UNSUPPORTED, "input contains NaN or infinite coordinates");
+    if (S.min_cell[0] < 0 || S.min_cell[1] < 0 || S.min_cell[2] < -1)
+        return fail(XNYZ_ERR_UNSUPPORTED, "lattice index outside the int range (coordinates too large for the bound)");
+    const int rx = S.max_cell[0], ry = S.max_cell[1], rz = S.max_cell[2];
+    const bool defects = S.min_cell[2] < 0;  // truncated-octahedron cells at z = -1
+    const int max_range = std::max({rx, ry, rz});
+    const bool direct = max_range < prm.direct_threshold;
+
+    // ---- 2. key layout ----
+    BlockKeyParams bkp{};
+    DirectKeyParams dkp{};
+    int key_bits = 0;
+    const auto& hm = hilbert_machines();
+    if (direct) {
+        int bits = bitlen(static_cast<uint64_t>(max_range));
+        if (bits == 0) bits = 1;
+        if (bits > 20) return fail(XNYZ_ERR_UNSUPPORTED, "direct mode with more than 20 bits per axis");
+        dkp.bits = bits;
+        dkp.hilbert = hil;
+        if (defects) {
+            dkp.defect_flag = 1ull << (3 * (bits + 1));
+            dkp.defect_high = (spread3_host(0x1fffffu) << 2) & ~(dkp.defect_flag - 1);
+            key_bits = 3 * (bits + 1) + 1;
+        } else {
+            key_bits = 3 * bits;
+        }
+    } else {
+        const unsigned __int128 nx = static_cast<uint64_t>(rx) / 128 + 1, ny = static_cast<uint64_t>(ry) / 128 + 1,
+                                nz = static_cast<uint64_t>(rz) / 128 + 1;
+        const unsigned __int128 cells = nx * ny * nz;
+        if (cells > (static_cast<unsigned __int128>(1) << 43))
+            return fail(XNYZ_ERR_UNSUPPORTED, "block ids need more than 43 bits");
+        const int B = bitlen(static_cast<uint64_t>(cells - 1));
+        bkp.nx = static_cast<uint64_t>(nx);
+        bkp.ny = static_cast<uint64_t>(ny);
+        bkp.hilbert = hil;
+        bkp.hstart = hm.fwd_block_start;
+        key_bits = B + 21;
+        if (defects) {
+            // z = -1 wraps to 2^64 - 1 before the division by 64 (block_quantizer.hpp:103):
+            // their ids are ((2^58 - 1) / 2) * nx * ny + (cx/2 + cy/2 * nx) modulo 2^64.
+            const uint64_t base = ((~0ull >> 6) >> 1) * (static_cast<uint64_t>(nx) * static_cast<uint64_t>(ny));
+            const unsigned __int128 top = static_cast<unsigned __int128>(base) + nx * ny;
+            if (static_cast<unsigned __int128>(base) < cells || top > (static_cast<unsigned __int128>(1) << 64))
+                return fail(XNYZ_ERR_UNSUPPORTED, "z = -1 cells whose block ids interleave the others");
+            bkp.defect_base = base;
+            bkp.defect_flag = 1ull << (B + 21);
+            key_bits = B + 22;
+        }
+        if (key_bits > 64) return fail(XNYZ_ERR_UNSUPPORTED, "sort keys wider than 64 bits");
+    }
+    const int passes = static_cast<int>(cdiv(key_bits, 8));
+
+    // ---- 3. arena plan ----
+    const CPlan cp = make_cplan(n, want_order, arena_reserved);
+    const uint64_t tiles = cp.tiles;
+    const size_t o_k0 = cp.o_k0, o_k1 = cp.o_k1, o_v0 = cp.o_v0, o_v1 = cp.o_v1, o_rep = cp.o_rep, o_quad = cp.o_quad,
+                 o_patch = cp.o_patch, o_blkid = cp.o_blkid, o_blkunit = cp.o_blkunit, o_unitpos = cp.o_unitpos,
+                 o_counts = cp.o_counts, o_over_v = cp.o_over_v, o_over_u = cp.o_over_u, o_dblk = cp.o_dblk,
+                 o_dcnt = cp.o_dcnt;
+    const LB lb_units = cp.lb_units, lb_enc = cp.lb_enc;
+    Plan pl;
+    pl.total = cp.total;
+    (void)tiles;
+    TRY(ensure_arena(c, pl.total));
+
+    // ---- 4. keys + digit histograms ----
+    SortBufs sb{{at<unsigned long long>(c, o_k0), at<unsigned long long>(c, o_k1)},
+                {want_order ? at<uint32_t>(c, o_v0) : nullptr, want_order ? at<uint32_t>(c, o_v1) : nullptr}};
+    TRY(memset_small(c, offsetof(Small, sort_hist), sizeof(uint32_t) * 8 * 256, 0));
+    CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_fwd, hm.fwd.data(), 256, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_inv, hm.inv.data(), 256, cudaMemcpyHostToDevice, st));
+    if (direct)
+        launch_keys_direct(d_xyz, n, q, SMALL_FIELD(c, stats), dkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
+                           passes, c->d_small->sort_hist, st);
+    else
+        launch_keys_block(d_xyz, n, q, SMALL_FIELD(c, stats), bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0], passes,
+                          c->d_small->sort_hist, st);
+    int res = 0;
+    TRY(radix_sort(c, sb, n, passes, c->d_small->sort_hist, res));
+    const unsigned long long* sorted = sb.keys[res];
+    if (want_order) R.d_order = sb.vals[res];
+
+    // ---- 5. units ----
+    TRY(memset_small(c, offsetof(Small, counters), sizeof(unsigned long long) * 8, 0));
+    TRY(memset_small(c, offsetof(Small, hist_rep), sizeof(unsigned long long) * 256, 0));
+    TRY(memset_small(c, offsetof(Small, first_rep), sizeof(uint32_t) * 256, 0xff));
+    TRY(memset_small(c, offsetof(Small, hist_quad), sizeof(unsigned long long) * 256, 0));
+    TRY(memset_small(c, offsetof(Small, first_quad), sizeof(uint32_t) * 256, 0xff));
+    TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 64, 0));
+    TRY(lb_clear(c, lb_units, 3));
+    UnitOutputs uo;
+    uo.rep_sym = at<uint8_t>(c, o_rep);
+    uo.quad_sym = at<uint8_t>(c, o_quad);
+    uo.patches = at<unsigned long long>(c, o_patch);
+    uo.blk_id = at<unsigned long long>(c, o_blkid);
+    uo.blk_unit = at<uint32_t>(c, o_blkunit);
+    uo.unit_pos = at<uint32_t>(c, o_unitpos);
+    uo.hist_rep = c->d_small->hist_rep;
+    uo.first_rep = c->d_small->first_rep;
+    uo.hist_quad = c->d_small->hist_quad;
+    uo.first_quad = c->d_small->first_quad;
+    uo.counters = c->d_small->counters;
+    if (direct)
+        launch_units_direct(sorted, n, rle, dkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
+                            SMALL_FIELD(c, err), st);
+    else
+        launch_units_block(sorted, n, rle, bkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
+                           SMALL_FIELD(c, err), st);
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, counters), sizeof(unsigned long long) * 8));
+    const uint64_t U = c->h_small->counters[0], P = c->h_small->counters[1], NB = c->h_small->counters[2];
+    const uint64_t psum = c->h_small->counters[3];
+    TRY(check_device_errors(c));
+
+    // ---- 6. count and block statistics ----
+    if (rle) {
+        TRY(memset_small(c, offsetof(Small, cnt_hist), sizeof(unsigned long long) * kCountDense, 0));
+        TRY(memset_small(c, offsetof(Small, cnt_first), sizeof(uint32_t) * kCountDense, 0xff));
+        TRY(memset_small(c, offsetof(Small, over_n), sizeof(uint32_t), 0));
+        CountStats cs{c->d_small->cnt_hist, c->d_small->cnt_first, at<uint32_t>(c, o_over_v), at<uint32_t>(c, o_over_u),
+                      SMALL_FIELD(c, over_n)};
+        launch_count_stats(uo.unit_pos, U, n, at<int32_t>(c, o_counts), cs, st);
+    }
+    if (!direct) {
+        TRY(memset_small(c, offsetof(Small, max2), sizeof(unsigned long long) * 2, 0));
+        launch_block_deltas(uo.blk_id, uo.blk_unit, NB, U, at<unsigned long long>(c, o_dblk),
+                            at<unsigned long long>(c, o_dcnt), c->d_small->max2, st);
+    }
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, hist_rep),
+                    offsetof(Small, tile_counters) - offsetof(Small, hist_rep)));  // hists, counts, maxima
+    const Small& H = *c->h_small;
+
+    // ---- 7. codebooks (host replay of the reference's container order) ----
+    std::vector<SymbolStat> st_rep, st_quad, st_cnt;
+    for (int s = 0; s < 256; ++s) {
+        if (H.hist_rep[s]) st_rep.push_back(SymbolStat{static_cast<uint64_t>(s), H.hist_rep[s], H.first_rep[s]});
+        if (!direct && H.hist_quad[s])
+            st_quad.push_back(SymbolStat{static_cast<uint64_t>(s), H.hist_quad[s], H.first_quad[s]});
+    }
+    const StreamCode code_rep = build_stream_code(SymType::U64, st_rep, U);
+    StreamCode code_quad;
+    if (!direct) code_quad = build_stream_code(SymType::U8, st_quad, U);
+    StreamCode code_cnt;
+    std::vector<uint32_t> sparse_val, sparse_bits;
+    std::vector<uint8_t> sparse_len;
+    std::vector<uint32_t> dense_bits(kCountDense, 0);
+    std::vector<uint8_t> dense_len(kCountDense, 0);
+    if (rle) {
+        for (int v = 0; v < kCountDense; ++v)
+            if (H.cnt_hist[v]) st_cnt.push_back(SymbolStat{static_cast<uint64_t>(v), H.cnt_hist[v], H.cnt_first[v]});
+        const uint32_t over = H.over_n;
+        if (over) {
+            std::vector<uint32_t> ov(over), ou(over);
+            CUDA_TRY(cudaMemcpyAsync(ov.data(), at<uint32_t>(c, o_over_v), 4ull * over, cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaMemcpyAsync(ou.data(), at<uint32_t>(c, o_over_u), 4ull * over, cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            std::unordered_map<uint32_t, std::pair<uint64_t, uint64_t>> agg;  // value -> (count, first unit)
+            for (uint32_t i = 0; i < over; ++i) {
+                auto& e = agg[ov[i]];
+                if (e.first == 0) e.second = ou[i];
+                e.first += 1;
+                e.second = std::min<uint64_t>(e.second, ou[i]);
+            }
+            for (auto& kv : agg) st_cnt.push_back(SymbolStat{kv.first, kv.second.first, kv.second.second});
+        }
+        code_cnt = build_count_code(st_cnt, U);
+        if (!code_cnt.exp_golomb) {
+            std::vector<std::pair<uint32_t, size_t>> sp;
+            for (size_t i = 0; i < code_cnt.symbols.size(); ++i) {
+                const uint32_t v = static_cast<uint32_t>(code_cnt.symbols[i]);
+                if (v < static_cast<uint32_t>(kCountDense)) {
+                    dense_bits[v] = code_cnt.codes[i].bits;
+                    dense_len[v] = code_cnt.codes[i].len;
+                } else {
+                    sp.emplace_back(v, i);
+                }
+            }
+            std::sort(sp.begin(), sp.end());
+            for (auto& e : sp) {
+                sparse_val.push_back(e.first);
+                sparse_bits.push_back(code_cnt.codes[e.second].bits);
+                sparse_len.push_back(code_cnt.codes[e.second].len);
+            }
+        }
+    }
+    auto to_bytecodes = [](const StreamCode& sc) {
+        ByteCodes b{};
+        for (size_t i = 0; i < sc.symbols.size(); ++i) {
+            const uint64_t s = sc.symbols[i];
+            if (s < 256) {
+                b.bits[s] = sc.codes[i].bits;
+                b.len[s] = sc.codes[i].len;
+            }
+        }
+        return b;
+    };
+    c->h_small->codes[0] = to_bytecodes(code_rep);
+    c->h_small->codes[1] = to_bytecodes(code_quad);
+    CUDA_TRY(cudaMemcpyAsync(c->d_small->codes, c->h_small->codes, sizeof(ByteCodes) * 2, cudaMemcpyHostToDevice, st));
+    const uint8_t grk = golomb_rice_k(psum, P, false);
+    int w_blk = 1, w_cnt = 1;
+    if (!direct) {
+        w_blk = H.max2[0] == 0 ? 1 : bitlen(H.max2[0]);
+        w_cnt = H.max2[1] == 0 ? 1 : bitlen(H.max2[1]);
+    }
+
+    // ---- 8. encoders ----
+    // Output sizes: Huffman and bit-pack streams are known exactly; the Golomb-Rice stream is
+    // bounded by P*(k+1) + sum(v >> k) <= P*(k+1) + (sum >> k) + P.
+    const uint64_t bits_rep = code_rep.encoded_bits, bits_quad = direct ? 0 : code_quad.encoded_bits;
+    const uint64_t bits_cnt = rle ? code_cnt.encoded_bits : 0;
+    const unsigned __int128 gr_bound = static_cast<unsigned __int128>(P) * (grk + 2) + (psum >> grk);
+    if (gr_bound > (static_cast<unsigned __int128>(1) << 40))
+        return fail(XNYZ_ERR_UNSUPPORTED, "Golomb-Rice stream larger than 2^40 bits");
+    const uint64_t bits_gr = static_cast<uint64_t>(gr_bound);
+    auto words_for = [](uint64_t bits) { return cdiv(bits, 32) + 4; };
+    Plan pe;
+    pe.total = pl.total;
+    const size_t o_w_blk = pe.add(4 * words_for(NB * static_cast<uint64_t>(w_blk)));
+    const size_t o_w_cnt = pe.add(4 * words_for(NB * static_cast<uint64_t>(w_cnt)));
+    const size_t o_w_gr = pe.add(4 * words_for(bits_gr));
+    const size_t o_w_rep = pe.add(4 * words_for(bits_rep));
+    const size_t o_w_quad = pe.add(4 * words_for(bits_quad));
+    const size_t o_w_cn = pe.add(4 * words_for(bits_cnt));
+    const size_t o_dense = pe.add(kCountDense * 5);
+    const size_t o_sparse = pe.add(sparse_val.size() * 9 + 16);
+    const size_t enc_begin = o_w_blk, enc_end = pe.total;
+    if (pe.total > c->arena.cap) {
+        // Growing would move the arena; the inputs above live in it.  Plan for the worst
+        // case next time and redo this call.
+        return fail(XNYZ_ERR_OOM, "__grow__:" + std::to_string(pe.total));
+    }
+    CUDA_TRY(cudaMemsetAsync(c->arena.base + enc_begin, 0, enc_end - enc_begin, st));
+    TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
+    TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 64, 0));
+    TRY(lb_clear(c, lb_enc, 4));
+    const LookBackState lbs = lb_state(c, lb_enc);
+    auto chan = [&](int ch) {
+        return LookBackState{lbs.flag + ch * lb_enc.tiles, lbs.agg + ch * lb_enc.tiles, lbs.inc + ch * lb_enc.tiles};
+    };
+    if (!direct) {
+        launch_bitpack(at<unsigned long long>(c, o_dblk), NB, w_blk, at<uint32_t>(c, o_w_blk), st);
+        launch_bitpack(at<unsigned long long>(c, o_dcnt), NB, w_cnt, at<uint32_t>(c, o_w_cnt), st);
+    }
+    launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
+                     SMALL_FIELD(c, tile_counters[0]),
+                     SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), st);
+    if (!code_rep.exp_golomb)
+        launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
+                              chan(1),
+                              SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err), st);
+    if (!direct)
+        launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
+                              32 * words_for(bits_quad), chan(2),
+                              SMALL_FIELD(c, tile_counters[2]), SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), st);
+    if (rle) {
+        uint32_t* dbits = at<uint32_t>(c, o_dense);
+        uint8_t* dlen = reinterpret_cast<uint8_t*>(dbits + kCountDense);
+        uint32_t* sval = at<uint32_t>(c, o_sparse);
+        uint32_t* sbits = sval + sparse_val.size();
+        uint8_t* slen = reinterpret_cast<uint8_t*>(sbits + sparse_val.size());
+        CUDA_TRY(cudaMemcpyAsync(dbits, dense_bits.data(), 4 * kCountDense, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(dlen, dense_len.data(), kCountDense, cudaMemcpyHostToDevice, st));
+        if (!sparse_val.empty()) {
+            CUDA_TRY(cudaMemcpyAsync(sval, sparse_val.data(), 4 * sparse_val.size(), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(sbits, sparse_bits.data(), 4 * sparse_val.size(), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(slen, sparse_len.data(), sparse_val.size(), cudaMemcpyHostToDevice, st));
+        }
+        launch_count_encode(at<int32_t>(c, o_counts), U, code_cnt.exp_golomb ? code_cnt.eg_k : -1, dbits, dlen, sval,
+                            sbits, slen, static_cast<uint32_t>(sparse_val.size()), at<uint32_t>(c, o_w_cn),
+                            32 * words_for(bits_cnt), chan(3),
+                            SMALL_FIELD(c, tile_counters[3]), SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), st);
+    }
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8));
+    TRY(check_device_errors(c));
+    const uint64_t gr_bits = c->h_small->totals[0];
+    if (!code_rep.exp_golomb && c->h_small->totals[1] != bits_rep)
+        return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (repos)");
+    if (!direct && c->h_small->totals[2] != bits_quad) return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (quads)");
+    if (rle && c->h_small->totals[3] != bits_cnt) return fail(XNYZ_ERR_CUDA, "count encoder size mismatch");
+
+    // ---- 9. container (Appendix: block_compressor.hpp:56-215, block_compressor_rle.hpp:125-314) ----
+    Container& K = R.cont;
+    K.pod<uint64_t>(U);
+    K.pod<uint64_t>(0);  // params.size(): the cube and truncated-octahedron quantizers have none
+    K.pod<int32_t>(rx);
+    K.pod<int32_t>(ry);
+    K.pod<int32_t>(rz);
+    K.pod<uint8_t>(hil ? 1 : 0);
+    K.pod<uint8_t>(direct ? 1 : 0);
+    const std::vector<uint8_t> gr_meta = P ? le5(static_cast<uint32_t>(P), grk) : std::vector<uint8_t>{};
+    if (direct) {
+        K.stream(gr_meta, at<uint32_t>(c, o_w_gr), P ? cdiv(gr_bits, 8) : 0);
+        K.stream(code_rep.meta, at<uint32_t>(c, o_w_rep), cdiv(bits_rep, 8));
+    } else {
+        K.stream(le5(static_cast<uint32_t>(NB), static_cast<uint8_t>(w_blk)), at<uint32_t>(c, o_w_blk),
+                 cdiv(NB * static_cast<uint64_t>(w_blk), 8));
+        K.stream(le5(static_cast<uint32_t>(NB), static_cast<uint8_t>(w_cnt)), at<uint32_t>(c, o_w_cnt),
+                 cdiv(NB * static_cast<uint64_t>(w_cnt), 8));
+        K.stream(gr_meta, at<uint32_t>(c, o_w_gr), P ? cdiv(gr_bits, 8) : 0);
+        K.stream(code_rep.meta, at<uint32_t>(c, o_w_rep), cdiv(bits_rep, 8));
+        K.stream({}, nullptr, 0);  // quad patches: quad deltas are < 8, never patched
+        K.stream(code_quad.meta, at<uint32_t>(c, o_w_quad), cdiv(bits_quad, 8));
+    }
+    if (rle) K.stream(code_cnt.meta, at<uint32_t>(c, o_w_cn), cdiv(bits_cnt, 8));
+    K.pod<float>(S.offset[0]);
+    K.pod<float>(S.offset[1]);
+    K.pod<float>(S.offset[2]);
+
+    xnyz_compress_info& I = R.info;
+    I.num_points = n;
+    I.num_units = U;
+    I.num_blocks = direct ? 0 : NB;
+    I.num_patches = P;
+    I.container_bytes = K.skel.size();
+    I.range[0] = rx;
+    I.range[1] = ry;
+    I.range[2] = rz;
+    I.is_direct = direct;
+    I.counts_exp_golomb = rle && code_cnt.exp_golomb;
+    float emax;
+    std::memcpy(&emax, &S.mse_max_bits, 4);
+    I.max_l2_error = std::sqrt(static_cast<double>(emax));
+    I.mse = S.mse_sum / static_cast<double>(n);
+    return XNYZ_OK;
+}
+
+// Runs compress_core, growing the arena and retrying once when the encoders need more.
+xnyz_status compress_run(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& p, bool want_order,
+                         size_t reserved, CompressOut& R) {
+    xnyz_status s = compress_core(c, d_xyz, n, p, want_order, reserved, R);
+    if (s == XNYZ_ERR_OOM && g_last_error.rfind("__grow__:", 0) == 0) {
+        const size_t need = std::stoull(g_last_error.substr(9));
+        // Input points may live in the arena's reserved prefix: keep them.
+        if (reserved) {
+            char* old = c->arena.base;
+            char* fresh = nullptr;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            CUDA_TRY(cudaMalloc(&fresh, align_up(need + need / 8, 1 << 20)));
+            CUDA_TRY(cudaMemcpyAsync(fresh, old, reserved, cudaMemcpyDeviceToDevice, c->stream));
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            cudaFree(old);
+            const ptrdiff_t shift = fresh - old;
+            c->arena.base = fresh;
+            c->arena.cap = align_up(need + need / 8, 1 << 20);
+            d_xyz = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d_xyz) + shift);
+        } else {
+            TRY(ensure_arena(c, need));
+        }
+        R = CompressOut{};
+        s = compress_core(c, d_xyz, n, p, want_order, reserved, R);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- header parse -----------
+struct StreamRef {
+    uint64_t meta_off = 0, meta_len = 0, data_off = 0, data_len = 0;
+    std::vector<uint8_t> meta;
+};
+struct Header {
+    uint64_t units = 0;
+    int32_t rx = 0, ry = 0, rz = 0;
+    bool hilbert = false, direct = false;
+    std::vector<StreamRef> streams;
+    float off[3] = {0, 0, 0};
+};
+
+// Reads the container layout (block_decompressor.hpp:40-176, block_decompressor_rle.hpp:41-202)
+// through `rd(offset, bytes, dst)`.
+template <typename Read>
+xnyz_status parse_header(Read rd, uint64_t len, bool rle, Header& h) {
+    uint64_t p = 0;
+    auto get = [&](void* dst, uint64_t bytes) -> bool {
+        if (bytes > len || p > len - bytes) return false;
+        if (!rd(p, bytes, dst)) return false;
+        p += bytes;
+        return true;
+    };
+    uint64_t np = 0;
+    uint8_t hb = 0, db = 0;
+    if (!get(&h.units, 8) || !get(&np, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    if (np > (len - p) / 4) return fail(XNYZ_ERR_BAD_STREAM, "bad parameter count");
+    p += 4 * np;  // quantizer parameters (none for cube / truncated octahedron)
+    if (!get(&h.rx, 4) || !get(&h.ry, 4) || !get(&h.rz, 4) || !get(&hb, 1) || !get(&db, 1))
+        return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    h.hilbert = hb != 0;
+    h.direct = db != 0;
+    const int ns = (h.direct ? 2 : 6) + (rle ? 1 : 0);
+    for (int i = 0; i < ns; ++i) {
+        StreamRef s;
+        if (!get(&s.data_len, 8) || !get(&s.meta_len, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated stream header");
+        if (s.meta_len > len - p) return fail(XNYZ_ERR_BAD_STREAM, "truncated stream meta");
+        s.meta_off = p;
+        s.meta.resize(s.meta_len);
+        if (s.meta_len && !get(s.meta.data(), s.meta_len)) return fail(XNYZ_ERR_BAD_STREAM, "truncated stream meta");
+        if (s.data_len > len - p) return fail(XNYZ_ERR_BAD_STREAM, "truncated stream data");
+        s.data_off = p;
+        p += s.data_len;
+        h.streams.push_back(std::move(s));
+    }
+    if (!get(h.off, 12)) return fail(XNYZ_ERR_BAD_STREAM, "truncated offset");
+    return XNYZ_OK;
+}
+
+uint32_t le32(const std::vector<uint8_t>& m) {
+    return static_cast<uint32_t>(m[0]) | (static_cast<uint32_t>(m[1]) << 8) | (static_cast<uint32_t>(m[2]) << 16) |
+           (static_cast<uint32_t>(m[3]) << 24);
+}
+
+// Host-built decode tables of one Huffman stream.
+struct HuffTables {
+    int root_bits = 1;
+    int max_len = 0;
+    std::vector<uint32_t> root, tree;
+    std::vector<unsigned long long> symvals;
+};
+
+xnyz_status build_huff_tables(const ParsedMeta& pm, HuffTables& t) {
+    t = HuffTables{};
+    for (const auto& c : pm.codes) t.max_len = std::max<int>(t.max_len, c.len);
+    if (t.max_len > 32) return fail(XNYZ_ERR_UNSUPPORTED, "Huffman codes longer than 32 bits");
+    if (pm.symbols.size() >= (1u << 24)) return fail(XNYZ_ERR_UNSUPPORTED, "Huffman alphabet too large");
+    t.root_bits = std::max(1, std::min(t.max_len, 11));
+    const int rb = t.root_bits;
+    t.root.assign(1u << rb, 0u);
+    t.symvals.assign(pm.symbols.begin(), pm.symbols.end());
+    // Longer codes first so that a shorter code sharing a prefix wins, as the reference's
+    // bit-by-bit matcher stops at the first (shortest) match.
+    std::vector<size_t> order(pm.codes.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return pm.codes[a].len > pm.codes[b].len; });
+    for (size_t oi : order) {
+        const CodeEntry& ce = pm.codes[oi];
+        const int len = ce.len;
+        if (len == 0) continue;
+        const uint32_t bits = len >= 32 ? ce.bits : (ce.bits & ((1u << len) - 1u));
+        if (len <= rb) {
+            const uint32_t first = bits << (rb - len), span = 1u << (rb - len);
+            for (uint32_t k = 0; k < span; ++k) t.root[first + k] = (static_cast<uint32_t>(len) << 24) | static_cast<uint32_t>(oi);
+        } else {
+            const uint32_t top = bits >> (len - rb);
+            uint32_t& e = t.root[top];
+            uint32_t node;
+            if (e == 0u) {
+                node = static_cast<uint32_t>(t.tree.size() / 2);
+                t.tree.push_back(0xffffffffu);
+                t.tree.push_back(0xffffffffu);
+                e = 0x80000000u | node;
+            } else if (e & 0x80000000u) {
+                node = e & 0x7fffffffu;
+            } else {
+                continue;  // shadowed by a shorter code
+            }
+            bool shadowed = false;
+            for (int i = len - rb - 1; i >= 1; --i) {
+                const uint32_t b = (bits >> i) & 1u;
+                uint32_t& ch = t.tree[2 * node + b];
+                if (ch == 0xffffffffu) {
+                    const uint32_t nn = static_cast<uint32_t>(t.tree.size() / 2);
+                    t.tree.push_back(0xffffffffu);
+                    t.tree.push_back(0xffffffffu);
+                    t.tree[2 * node + b] = nn;
+                    node = nn;
+                } else if (ch & 0x80000000u) {
+                    shadowed = true;
+                    break;
+                } else {
+                    node = ch;
+                }
+            }
+            if (shadowed) continue;
+            uint32_t& leaf = t.tree[2 * node + (bits & 1u)];
+            if (leaf == 0xffffffffu) leaf = 0x80000000u | static_cast<uint32_t>(oi);
+        }
+    }
+    if (t.tree.empty()) t.tree.assign(2, 0xffffffffu);
+    return XNYZ_OK;
+}
+
+struct DecodeJob {
+    int kind = 0;
+    const uint32_t* words = nullptr;
+    uint64_t base_bits = 0, total_bits = 0, nsym = 0;
+    int width = 1;
+    void* out = nullptr;
+    DecodeTable table{};
+    int L = 1;
+    int slot = 0;
+    bool fill = false;
+    uint64_t fill_value = 0;
+};
+
+xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, const Header& h, int quantizer,
+                            float l2, bool rle, size_t reserved, float** d_out, uint64_t* n_out) {
+    cudaStream_t st = c->stream;
+    const QuantParams q = make_quant(quantizer, l2);
+    const uint64_t U = h.units;
+    if (U >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 cells");
+    const auto& hm = hilbert_machines();
+    auto words_of = [&](const StreamRef& s, uint64_t& base) {
+        base = (s.data_off & 3u) * 8u;
+        return reinterpret_cast<const uint32_t*>(d_cont + (s.data_off & ~static_cast<uint64_t>(3)));
+    };
+
+    // ---- stream metas ----
+    const int i_gr = h.direct ? 0 : 2, i_sym = h.direct ? 1 : 3;
+    const StreamRef& s_gr = h.streams[i_gr];
+    const StreamRef& s_sym = h.streams[i_sym];
+    uint64_t P = 0;
+    uint8_t grk = 0;
+    if (!(s_gr.meta.empty() && s_gr.data_len == 0)) {
+        if (s_gr.meta.size() != 5) return fail(XNYZ_ERR_BAD_STREAM, "Invalid meta size in Golomb-Rice packed data");
+        P = le32(s_gr.meta);
+        grk = s_gr.meta[4];
+        if (P && grk >= 63) return fail(XNYZ_ERR_BAD_STREAM, "Invalid k_param in Golomb-Rice packed data meta");
+    }
+    std::string perr;
+    ParsedMeta pm_sym, pm_quad, pm_cnt;
+    if (!parse_meta(SymType::U64, s_sym.meta.data(), s_sym.meta.size(), pm_sym, perr))
+        return fail(XNYZ_ERR_BAD_STREAM, perr);
+    uint64_t NB = 0;
+    int w_blk = 0, w_cnt = 0;
+    if (!h.direct) {
+        const StreamRef& sb = h.streams[0];
+        const StreamRef& sc = h.streams[1];
+        if (sb.meta.size() != 5 || sc.meta.size() != 5) return fail(XNYZ_ERR_BAD_STREAM, "Invalid meta size in bitpacked data");
+        NB = le32(sb.meta);
+        w_blk = sb.meta[4];
+        w_cnt = sc.meta[4];
+        if (le32(sc.meta) != NB) return fail(XNYZ_ERR_BAD_STREAM, "block and count streams disagree");
+        if (w_blk > 64 || w_cnt > 64) return fail(XNYZ_ERR_UNSUPPORTED, "bit width above 64");
+        if (NB * static_cast<uint64_t>(w_blk) > sb.data_len * 8 || NB * static_cast<uint64_t>(w_cnt) > sc.data_len * 8)
+            return fail(XNYZ_ERR_BAD_STREAM, "truncated bit-packed stream");
+        const StreamRef& sqp = h.streams[4];
+        if (!(sqp.meta.empty() && sqp.data_len == 0)) {
+            if (sqp.meta.size() != 5) return fail(XNYZ_ERR_BAD_STREAM, "Invalid meta size in Golomb-Rice packed data");
+            if (le32(sqp.meta) != 0) return fail(XNYZ_ERR_UNSUPPORTED, "patched quad deltas (never produced by the encoder)");
+        }
+        if (!parse_meta(SymType::U8, h.streams[5].meta.data(), h.streams[5].meta.size(), pm_quad, perr))
+            return fail(XNYZ_ERR_BAD_STREAM, perr);
+        if (pm_quad.exp_golomb) return fail(XNYZ_ERR_UNSUPPORTED, "exp-Golomb quad stream");
+    }
+    if (pm_sym.exp_golomb) return fail(XNYZ_ERR_UNSUPPORTED, "exp-Golomb repos stream");
+    for (uint64_t s : pm_sym.symbols)
+        if (s > 255) return fail(XNYZ_ERR_UNSUPPORTED, "repos symbols above 255 (never produced by the encoder)");
+    const StreamRef* s_cnt = rle ? &h.streams.back() : nullptr;
+    if (rle && !parse_meta(SymType::I32, s_cnt->meta.data(), s_cnt->meta.size(), pm_cnt, perr))
+        return fail(XNYZ_ERR_BAD_STREAM, perr);
+
+    // ---- arena plan ----
+    Plan pl;
+    pl.total = reserved;
+    const size_t o_blkd = pl.add(8 * NB + 8), o_cntd = pl.add(8 * NB + 8), o_blk = pl.add(8 * NB + 8),
+                 o_cnt = pl.add(8 * NB + 8), o_start = pl.add(8 * NB + 8);
+    const size_t o_patch = pl.add(8 * P + 8);
+    const size_t o_rep = pl.add(U + 8), o_quad = pl.add(U + 8), o_isst = pl.add(U + 8), o_stb = pl.add(4 * U + 8);
+    const size_t o_counts = pl.add(4 * U + 8);
+    const LB lb_scan = plan_lb(pl, cdiv(std::max<uint64_t>(NB, 1), kScanTile), 3);
+    struct TabOff {
+        size_t root, tree, sym;
+    };
+    HuffTables ht_sym, ht_quad, ht_cnt;
+    TRY(build_huff_tables(pm_sym, ht_sym));
+    if (!h.direct) TRY(build_huff_tables(pm_quad, ht_quad));
+    if (rle && !pm_cnt.exp_golomb) TRY(build_huff_tables(pm_cnt, ht_cnt));
+    auto plan_tab = [&](const HuffTables& t) {
+        return TabOff{pl.add(4 * t.root.size()), pl.add(4 * t.tree.size()), pl.add(8 * t.symvals.size() + 8)};
+    };
+    const TabOff to_sym = plan_tab(ht_sym), to_quad = plan_tab(ht_quad), to_cnt = plan_tab(ht_cnt);
+    // decode look-back state per stream (up to 4 streams)
+    auto dec_tiles = [](uint64_t bits) { return cdiv(cdiv(std::max<uint64_t>(bits, 1), kDecodeSubBits), kDecodeBlockSubs); };
+    const uint64_t dtiles = std::max({dec_tiles(s_gr.data_len * 8), dec_tiles(s_sym.data_len * 8),
+                                      h.direct ? 1 : dec_tiles(h.streams[5].data_len * 8),
+                                      rle ? dec_tiles(s_cnt->data_len * 8) : 1});
+    size_t o_dflag[4], o_dagg[4], o_dinc[4];
+    for (int i = 0; i < 4; ++i) {
+        o_dflag[i] = pl.add(4 * dtiles);
+        o_dagg[i] = pl.add(8 * dtiles * kDecodeMaxL);
+        o_dinc[i] = pl.add(16 * dtiles);
+    }
+    const uint64_t rtiles = cdiv(std::max<uint64_t>(U, 1), kScanTile);
+    const size_t o_rflag = pl.add(4 * rtiles * 5), o_ragg = pl.add(16 * rtiles * 5), o_rinc = pl.add(16 * rtiles * 5);
+    if (pl.total > c->arena.cap) return fail(XNYZ_ERR_OOM, "__grow__:" + std::to_string(pl.total));
+
+    TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
+    TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 64, 0));
+    TRY(memset_small(c, offsetof(Small, fallback), sizeof(uint32_t) * 8 * 2, 0));  // fallback + maxrun
+    TRY(memset_small(c, offsetof(Small, codewords), sizeof(unsigned long long) * 8, 0));
+    CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_inv, hm.inv.data(), 256, cudaMemcpyHostToDevice, st));
+    auto upload = [&](const HuffTables& t, const TabOff& o) -> xnyz_status {
+        if (!t.root.empty())
+            CUDA_TRY(cudaMemcpyAsync(at<uint32_t>(c, o.root), t.root.data(), 4 * t.root.size(), cudaMemcpyHostToDevice, st));
+        if (!t.tree.empty())
+            CUDA_TRY(cudaMemcpyAsync(at<uint32_t>(c, o.tree), t.tree.data(), 4 * t.tree.size(), cudaMemcpyHostToDevice, st));
+        if (!t.symvals.empty())
+            CUDA_TRY(cudaMemcpyAsync(at<unsigned long long>(c, o.sym), t.symvals.data(), 8 * t.symvals.size(),
+                                     cudaMemcpyHostToDevice, st));
+        return XNYZ_OK;
+    };
+    TRY(upload(ht_sym, to_sym));
+    TRY(upload(ht_quad, to_quad));
+    TRY(upload(ht_cnt, to_cnt));
+
+    // ---- block streams: bit-unpack + prefix sums ----
+    if (!h.direct && NB) {
+        uint64_t b0, b1;
+        const uint32_t* w0 = words_of(h.streams[0], b0);
+        const uint32_t* w1 = words_of(h.streams[1], b1);
+        launch_bitunpack(w0, b0, NB, w_blk, at<unsigned long long>(c, o_blkd), st);
+        launch_bitunpack(w1, b1, NB, w_cnt, at<unsigned long long>(c, o_cntd), st);
+        TRY(lb_clear(c, lb_scan, 3));
+        const LookBackState ls = lb_state(c, lb_scan);
+        auto ch = [&](int k) { return LookBackState{ls.flag + k * lb_scan.tiles, ls.agg + k * lb_scan.tiles, ls.inc + k * lb_scan.tiles}; };
+        launch_scan_u64(at<unsigned long long>(c, o_blkd), at<unsigned long long>(c, o_blk), NB, 0, ch(0),
+                        SMALL_FIELD(c, tile_counters[20]), nullptr, SMALL_FIELD(c, err), st);
+        launch_scan_u64(at<unsigned long long>(c, o_cntd), at<unsigned long long>(c, o_cnt), NB, 0, ch(1),
+                        SMALL_FIELD(c, tile_counters[21]), nullptr, SMALL_FIELD(c, err), st);
+        launch_scan_u64(at<unsigned long long>(c, o_cnt), at<unsigned long long>(c, o_start), NB, 1, ch(2),
+                        SMALL_FIELD(c, tile_counters[22]), SMALL_FIELD(c, count_total), SMALL_FIELD(c, err), st);
+        CUDA_TRY(cudaMemsetAsync(at<uint8_t>(c, o_isst), 0, U + 8, st));
+        launch_block_starts(at<unsigned long long>(c, o_start), NB, U, at<uint8_t>(c, o_isst), at<uint32_t>(c, o_stb),
+                            SMALL_FIELD(c, err), st);
+    }
+
+    // ---- entropy-coded streams ----
+    std::vector<DecodeJob> jobs;
+    auto huff_job = [&](const StreamRef& s, const ParsedMeta& pm, const HuffTables& t, const TabOff& o, int width,
+                        void* out, int slot) -> xnyz_status {
+        DecodeJob j;
+        j.kind = kCodeHuffman;
+        j.words = words_of(s, j.base_bits);
+        j.total_bits = s.data_len * 8;
+        j.nsym = U;
+        j.width = width;
+        j.out = out;
+        j.slot = slot;
+        if (U == 0) return XNYZ_OK;
+        if (pm.distinct == 0) return fail(XNYZ_ERR_BAD_STREAM, "empty Huffman table");
+        if (pm.distinct == 1) {  // decode(): one code -> every symbol is that symbol
+            j.fill = true;
+            j.fill_value = pm.symbols[0];
+        }
+        j.table.root = at<uint32_t>(c, o.root);
+        j.table.tree = at<uint32_t>(c, o.tree);
+        j.table.symvals = at<unsigned long long>(c, o.sym);
+        j.table.root_bits = t.root_bits;
+        j.L = std::max(1, t.max_len);
+        jobs.push_back(j);
+        return XNYZ_OK;
+    };
+    if (P) {
+        DecodeJob j;
+        j.kind = kCodeGolombRice;
+        j.words = words_of(s_gr, j.base_bits);
+        j.total_bits = s_gr.data_len * 8;
+        j.nsym = P;
+        j.width = 8;
+        j.out = at<unsigned long long>(c, o_patch);
+        j.table.param = grk;
+        j.slot = 0;
+        j.L = -1;  // from the longest one-run
+        jobs.push_back(j);
+    }
+    TRY(huff_job(s_sym, pm_sym, ht_sym, to_sym, 1, at<uint8_t>(c, o_rep), 1));
+    if (!h.direct) TRY(huff_job(h.streams[5], pm_quad, ht_quad, to_quad, 1, at<uint8_t>(c, o_quad), 2));
+    if (rle) {
+        if (pm_cnt.exp_golomb) {
+            DecodeJob j;
+            j.kind = kCodeExpGolomb;
+            j.words = words_of(*s_cnt, j.base_bits);
+            j.total_bits = s_cnt->data_len * 8;
+            j.nsym = U;
+            j.width = 4;
+            j.out = at<int32_t>(c, o_counts);
+            j.table.param = pm_cnt.eg_k;
+            j.table.zigzag = 1;
+            j.L = kDecodeMaxL;
+            j.slot = 3;
+            if (U) jobs.push_back(j);
+        } else {
+            TRY(huff_job(*s_cnt, pm_cnt, ht_cnt, to_cnt, 4, at<int32_t>(c, o_counts), 3));
+        }
+    }
+    for (auto& j : jobs) {
+        if (j.fill) {
+            if (j.width == 1)
+                launch_fill_u8(static_cast<uint8_t*>(j.out), j.nsym, static_cast<uint8_t>(j.fill_value), st);
+            else
+                launch_fill_u32(static_cast<uint32_t*>(j.out), j.nsym, static_cast<uint32_t>(j.fill_value), st);
+            continue;
+        }
+        const uint32_t* Lrun = nullptr;
+        if (j.kind == kCodeGolombRice) {
+            const uint64_t w_first = j.base_bits / 32, nw = cdiv(j.base_bits + j.total_bits, 32) - w_first;
+            launch_max_ones_run(j.words, nw, SMALL_FIELD(c, maxrun[j.slot]), st);
+            Lrun = SMALL_FIELD(c, maxrun[j.slot]);
+        }
+        CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_dflag[j.slot]), 0, 4 * dtiles, st));
+        launch_decode_stream(j.kind, j.words, j.base_bits, j.total_bits, j.table, j.L, Lrun, j.nsym, j.width, j.out,
+                             at<uint32_t>(c, o_dflag[j.slot]), at<unsigned long long>(c, o_dagg[j.slot]),
+                             at<unsigned long long>(c, o_dinc[j.slot]), SMALL_FIELD(c, tile_counters[30 + j.slot]),
+                             SMALL_FIELD(c, err), SMALL_FIELD(c, fallback[j.slot]), SMALL_FIELD(c, codewords[j.slot]),
+                             st);
+    }
+    CUDA_TRY(cudaGetLastError());
+    // count total (for -rle) after the count stream is decoded
+    TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
+    TRY(fetch_small(c, offsetof(Small, fallback), sizeof(uint32_t) * 8));
+    bool refetch = false;
+    for (auto& j : jobs) {
+        if (j.fill) continue;
+        if (c->h_small->fallback[j.slot]) {
+            launch_decode_sequential(j.kind, j.words, j.base_bits, j.total_bits, j.table, j.nsym, j.width, j.out,
+                                     SMALL_FIELD(c, codewords[j.slot]), SMALL_FIELD(c, err), st);
+            refetch = true;
+        }
+    }
+    (void)refetch;
+    if (rle && U) launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, totals), offsetof(Small, tile_counters) - offsetof(Small, totals)));
+    TRY(check_device_errors(c));
+    for (auto& j : jobs)
+        if (!j.fill && c->h_small->codewords[j.slot] < j.nsym)
+            return fail(XNYZ_ERR_BAD_STREAM, "stream holds fewer codes than points");
+    if (!h.direct && NB && c->h_small->count_total != U)
+        return fail(XNYZ_ERR_BAD_STREAM, "block counts do not add up to the point count");
+    if (!h.direct && NB == 0 && U) return fail(XNYZ_ERR_BAD_STREAM, "no blocks");
+    const uint64_t nout = rle ? c->h_small->totals[0] : U;
+
+    // ---- output buffer (after the arena's planned part) ----
+    Plan po;
+    po.total = pl.total;
+    const size_t o_out = po.add(12 * nout + 16);
+    if (po.total > c->arena.cap) return fail(XNYZ_ERR_OOM, "__grow__:" + std::to_string(po.total));
+
+    RecoverParams rp{};
+    rp.q = q;
+    rp.off[0] = h.off[0];
+    rp.off[1] = h.off[1];
+    rp.off[2] = h.off[2];
+    // nx uses the size_t conversion of the stored int range (block_quantizer.hpp:163)
+    rp.nx = static_cast<uint64_t>(static_cast<int64_t>(h.rx)) / 128 + 1;
+    rp.ny = static_cast<uint64_t>(static_cast<int64_t>(h.ry)) / 128 + 1;
+    rp.hilbert = h.hilbert;
+    rp.hstart_inv = hm.inv_block_start;
+    rp.rle = rle;
+    rp.direct = h.direct;
+    {
+        int mr = std::max({h.rx, h.ry, h.rz}), bits = 0;
+        for (int t = mr; t > 0; t >>= 1) ++bits;
+        if (bits == 0) bits = 1;
+        if (h.direct && bits > 20) return fail(XNYZ_ERR_UNSUPPORTED, "direct mode with more than 20 bits per axis");
+        rp.bits = bits;
+    }
+    RecoverInputs ri{};
+    ri.rep_sym = at<uint8_t>(c, o_rep);
+    ri.rep_patch = at<unsigned long long>(c, o_patch);
+    ri.npatch = P;
+    ri.quad_sym = at<uint8_t>(c, o_quad);
+    ri.is_start = at<uint8_t>(c, o_isst);
+    ri.start_block = at<uint32_t>(c, o_stb);
+    ri.blk_ids = at<unsigned long long>(c, o_blk);
+    ri.nblocks = NB;
+    ri.counts = at<int32_t>(c, o_counts);
+    CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_rflag), 0, 4 * rtiles * 5, st));
+    float* out = at<float>(c, o_out);
+    launch_recover_units(ri, U, nout, rp, c->d_small->hil_inv, at<uint32_t>(c, o_rflag),
+                         at<unsigned long long>(c, o_ragg), at<unsigned long long>(c, o_rinc),
+                         SMALL_FIELD(c, tile_counters[40]), out, SMALL_FIELD(c, err), st);
+    CUDA_TRY(cudaGetLastError());
+    TRY(check_device_errors(c));
+    *d_out = out;
+    *n_out = nout;
+    return XNYZ_OK;
+}
+
+xnyz_status decompress_run(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, const Header& h, int quantizer, float l2,
+                           bool rle, size_t reserved, float** d_out, uint64_t* n_out) {
+    // The container may live in the arena's reserved prefix; growing keeps that prefix.
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        xnyz_status s = decompress_core(c, d_cont, len, h, quantizer, l2, rle, reserved, d_out, n_out);
+        if (!(s == XNYZ_ERR_OOM && g_last_error.rfind("__grow__:", 0) == 0)) return s;
+        const size_t need = std::stoull(g_last_error.substr(9));
+        if (reserved) {
+            char* old = c->arena.base;
+            char* fresh = nullptr;
+            const size_t cap = align_up(need + need / 8, 1 << 20);
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            CUDA_TRY(cudaMalloc(&fresh, cap));
+            CUDA_TRY(cudaMemcpyAsync(fresh, old, reserved, cudaMemcpyDeviceToDevice, c->stream));
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            cudaFree(old);
+            d_cont = reinterpret_cast<const uint8_t*>(fresh + (reinterpret_cast<const char*>(d_cont) - old));
+            c->arena.base = fresh;
+            c->arena.cap = cap;
+        } else {
+            TRY(ensure_arena(c, need));
+        }
+    }
+    return fail(XNYZ_ERR_OOM, "workspace growth did not converge");
+}
+
+}  // namespace
+
+// ====================================================================== C ABI ==========
+extern "C" {
+
+const char* xnyz_last_error(void) { return g_last_error.c_str(); }
+const char* xnyz_version(void) { return "xnyzip-b200 0.1 (sm_100a)"; }
+
+xnyz_status xnyz_create(xnyz_ctx** out, int device, void* stream) {
+    if (!out) return fail(XNYZ_ERR_INVALID_ARG, "null context pointer");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(XNYZ_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(XNYZ_ERR_INVALID_ARG, "device index out of range");
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(XNYZ_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+    std::unique_ptr<xnyz_ctx> c(new xnyz_ctx());
+    c->device = device;
+    if (stream) {
+        c->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    CUDA_TRY(cudaMalloc(&c->d_small, sizeof(Small)));
+    CUDA_TRY(cudaMemset(c->d_small, 0, sizeof(Small)));
+    CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&c->h_small), sizeof(Small), cudaHostAllocDefault));
+    std::memset(c->h_small, 0, sizeof(Small));
+    CUDA_TRY(cudaEventCreate(&c->ev0));
+    CUDA_TRY(cudaEventCreate(&c->ev1));
+    (void)hilbert_machines();
+    *out = c.release();
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_destroy(xnyz_ctx* c) {
+    if (!c) return XNYZ_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->arena.base) cudaFree(c->arena.base);
+    if (c->sort_status) cudaFree(c->sort_status);
+    if (c->d_small) cudaFree(c->d_small);
+    if (c->h_small) cudaFreeHost(c->h_small);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->d_container) cudaFree(c->d_container);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_trim(xnyz_ctx* c) {
+    if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
+    cudaSetDevice(c->device);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->arena.base) cudaFree(c->arena.base);
+    c->arena = Arena{};
+    if (c->d_container) cudaFree(c->d_container);
+    c->d_container = nullptr;
+    c->d_container_cap = 0;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_set_zstd_library(const char* path) {
+    std::string err;
+    if (!zstd_load(path, err)) return fail(XNYZ_ERR_ZSTD, err);
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_host_alloc(void** ptr, size_t bytes) {
+    if (!ptr) return fail(XNYZ_ERR_INVALID_ARG, "null pointer");
+    CUDA_TRY(cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault));
+    return XNYZ_OK;
+}
+xnyz_status xnyz_host_free(void* ptr) {
+    if (ptr) CUDA_TRY(cudaFreeHost(ptr));
+    return XNYZ_OK;
+}
+
+void xnyz_free(void* p) { std::free(p); }
+
+xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_device, const xnyz_params* params,
+                          int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order,
+                          xnyz_compress_info* info) {
+    if (!c || !xyz || !params || !out || !out_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (use_zstd) {
+        std::string e;
+        if (!zstd_available(e)) return fail(XNYZ_ERR_ZSTD, e);
+    }
+    cudaStream_t st = c->stream;
+    CUDA_TRY(cudaEventRecord(c->ev0, st));
+    const float* d_xyz = xyz;
+    size_t reserved = 0;
+    if (!xyz_is_device) {
+        reserved = align_up(12 * n);
+        const bool wo = sort_order != nullptr && !params->rle;
+        TRY(ensure_arena(c, make_cplan(n, wo, reserved).total + encoder_reserve(n)));
+        CUDA_TRY(cudaMemcpyAsync(c->arena.base, xyz, 12 * n, cudaMemcpyHostToDevice, st));
+        d_xyz = reinterpret_cast<const float*>(c->arena.base);
+    }
+    CompressOut R;
+    const bool want_order = sort_order != nullptr && !params->rle;
+    TRY(compress_run(c, d_xyz, n, *params, want_order, reserved, R));
+    // container: skeleton on the host, stream bytes copied from the device into place
+    const size_t clen = R.cont.skel.size();
+    TRY(ensure_host_stage(c, clen));
+    std::memcpy(c->h_stage, R.cont.skel.data(), clen);
+    for (const Hole& hl : R.cont.holes)
+        CUDA_TRY(cudaMemcpyAsync(c->h_stage + hl.off, hl.dsrc, hl.bytes, cudaMemcpyDeviceToHost, st));
+    std::vector<uint32_t> order;
+    if (want_order) {
+        order.resize(n);
+        CUDA_TRY(cudaMemcpyAsync(order.data(), R.d_order, 4 * n, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaEventRecord(c->ev1, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (want_order)
+        for (uint64_t i = 0; i < n; ++i) sort_order[i] = order[i];
+    uint8_t* buf = nullptr;
+    uint64_t blen = 0;
+    if (use_zstd) {
+        std::string e;
+        const size_t cap = zstd_bound(clen);
+        buf = static_cast<uint8_t*>(std::malloc(cap ? cap : 1));
+        if (!buf) return fail(XNYZ_ERR_OOM, "host allocation");
+        size_t w = 0;
+        if (!zstd_compress_into(c->h_stage, clen, 3, buf, cap, w, e)) {
+            std::free(buf);
+            return fail(XNYZ_ERR_ZSTD, e);
+        }
+        blen = w;
+    } else {
+        buf = static_cast<uint8_t*>(std::malloc(clen ? clen : 1));
+        if (!buf) return fail(XNYZ_ERR_OOM, "host allocation");
+        std::memcpy(buf, c->h_stage, clen);
+        blen = clen;
+    }
+    *out = buf;
+    *out_len = blen;
+    if (info) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        R.info.gpu_ms = ms;
+        R.info.output_bytes = blen;
+        *info = R.info;
+    }
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, const xnyz_params* params,
+                                 const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info) {
+    if (!c || !xyz || !params || !dev_container || !container_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    CUDA_TRY(cudaEventRecord(c->ev0, st));
+    CompressOut R;
+    TRY(ensure_arena(c, make_cplan(n, false, 0).total + encoder_reserve(n)));
+    TRY(compress_run(c, xyz, n, *params, false, 0, R));
+    const size_t clen = R.cont.skel.size();
+    if (c->d_container_cap < clen + 64) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        if (c->d_container) cudaFree(c->d_container);
+        c->d_container = nullptr;
+        const size_t want = align_up(clen + clen / 4 + 64, 1 << 20);
+        CUDA_TRY(cudaMalloc(&c->d_container, want));
+        c->d_container_cap = want;
+    }
+    TRY(ensure_host_stage(c, clen));
+    std::memcpy(c->h_stage, R.cont.skel.data(), clen);
+    CUDA_TRY(cudaMemcpyAsync(c->d_container, c->h_stage, clen, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(c->d_container + clen, 0, 64, st));
+    for (const Hole& hl : R.cont.holes)
+        CUDA_TRY(cudaMemcpyAsync(c->d_container + hl.off, hl.dsrc, hl.bytes, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaEventRecord(c->ev1, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *dev_container = c->d_container;
+    *container_len = clen;
+    if (info) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        R.info.gpu_ms = ms;
+        R.info.output_bytes = clen;
+        *info = R.info;
+    }
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                            float l2_bound, int rle, float** xyz, uint64_t* n) {
+    if (!c || !in || !xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const uint8_t* raw = in;
+    uint64_t len = in_len;
+    std::string e;
+    if (is_zstd) {
+        uint64_t fs = 0;
+        if (!zstd_content_size(in, in_len, fs, e)) return fail(XNYZ_ERR_ZSTD, e);
+        TRY(ensure_host_stage(c, fs + 64));
+        if (!zstd_decompress(in, in_len, c->h_stage, fs, e)) return fail(XNYZ_ERR_ZSTD, e);
+        raw = c->h_stage;
+        len = fs;
+    }
+    Header h;
+    TRY(parse_header([&](uint64_t off, uint64_t bytes, void* dst) { std::memcpy(dst, raw + off, bytes); return true; },
+                     len, rle != 0, h));
+    const size_t reserved = align_up(len + 64);
+    TRY(ensure_arena(c, reserved));
+    CUDA_TRY(cudaMemcpyAsync(c->arena.base, raw, len, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(c->arena.base + len, 0, 64, st));
+    float* d_out = nullptr;
+    uint64_t nout = 0;
+    TRY(decompress_run(c, reinterpret_cast<const uint8_t*>(c->arena.base), len, h, quantizer, l2_bound, rle != 0,
+                       reserved, &d_out, &nout));
+    float* host = static_cast<float*>(std::malloc(12 * nout + 4));
+    if (!host) return fail(XNYZ_ERR_OOM, "host allocation");
+    if (nout) CUDA_TRY(cudaMemcpyAsync(host, d_out, 12 * nout, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *xyz = host;
+    *n = nout;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, uint64_t len, int quantizer,
+                                   float l2_bound, int rle, const float** dev_xyz, uint64_t* n) {
+    if (!c || !dev_container || !dev_xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    // The kernels read up to 16 bytes past a stream's end; containers from
+    // xnyz_compress_device carry 64 bytes of padding.  Others are copied into the arena.
+    const uint8_t* d_cont = dev_container;
+    size_t reserved = 0;
+    if (dev_container != c->d_container) {
+        reserved = align_up(len + 64);
+        TRY(ensure_arena(c, reserved));
+        CUDA_TRY(cudaMemcpyAsync(c->arena.base, dev_container, len, cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaMemsetAsync(c->arena.base + len, 0, 64, st));
+        d_cont = reinterpret_cast<const uint8_t*>(c->arena.base);
+    }
+    Header h;
+    xnyz_status s = parse_header(
+        [&](uint64_t off, uint64_t bytes, void* dst) {
+            return cudaMemcpyAsync(dst, d_cont + off, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+                   cudaStreamSynchronize(st) == cudaSuccess;
+        },
+        len, rle != 0, h);
+    if (s != XNYZ_OK) return s;
+    float* d_out = nullptr;
+    uint64_t nout = 0;
+    TRY(decompress_run(c, d_cont, len, h, quantizer, l2_bound, rle != 0, reserved, &d_out, &nout));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *dev_xyz = d_out;
+    *n = nout;
+    return XNYZ_OK;
+}
+
+// ---- stage entry points -------------------------------------------------------------------
+xnyz_status xnyz_stage_quantize(xnyz_ctx* c, const float* dev_xyz, uint64_t n, int quantizer, float l2_bound,
+                                float* offset3, int32_t* dev_cells) {
+    if (!c || !dev_xyz || !offset3 || !dev_cells || n == 0) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const QuantParams q = make_quant(quantizer, l2_bound);
+    PointStats init{};
+    for (int a = 0; a < 3; ++a) {
+        init.minkey[a] = ~0ull;
+        init.min_cell[a] = INT32_MAX;
+    }
+    c->h_small->stats = init;
+    CUDA_TRY(cudaMemcpyAsync(&c->d_small->stats, &c->h_small->stats, sizeof(PointStats), cudaMemcpyHostToDevice, c->stream));
+    launch_bbox(dev_xyz, n, SMALL_FIELD(c, stats), c->stream);
+    launch_quantize_range(dev_xyz, n, q, SMALL_FIELD(c, stats), 0, c->stream);
+    launch_quantize_cells(dev_xyz, n, q, SMALL_FIELD(c, stats), dev_cells, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    TRY(fetch_small(c, offsetof(Small, stats), sizeof(PointStats)));
+    for (int a = 0; a < 3; ++a) offset3[a] = c->h_small->stats.offset[a];
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_stage_recover(xnyz_ctx* c, const int32_t* dev_cells, uint64_t n, int quantizer, float l2_bound,
+                               const float* offset3, float* dev_xyz) {
+    if (!c || !dev_cells || !offset3 || !dev_xyz) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (int a = 0; a < 3; ++a) c->h_small->offset_in[a] = offset3[a];
+    CUDA_TRY(cudaMemcpyAsync(c->d_small->offset_in, c->h_small->offset_in, 12, cudaMemcpyHostToDevice, c->stream));
+    launch_recover_cells(dev_cells, n, make_quant(quantizer, l2_bound), c->d_small->offset_in, dev_xyz, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_stage_hilbert(xnyz_ctx* c, const uint64_t* dev_in, uint64_t n, unsigned iteration, int inverse,
+                               uint64_t* dev_out) {
+    if (!c || !dev_in || !dev_out) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    if (iteration > 20) return fail(XNYZ_ERR_UNSUPPORTED, "iteration above 20");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const auto& hm = hilbert_machines();
+    uint8_t* tab = inverse ? c->d_small->hil_inv : c->d_small->hil_fwd;
+    CUDA_TRY(cudaMemcpyAsync(tab, inverse ? hm.inv.data() : hm.fwd.data(), 256, cudaMemcpyHostToDevice, c->stream));
+    launch_hilbert(reinterpret_cast<const unsigned long long*>(dev_in), n, tab, static_cast<int>(iteration), 0u,
+                   reinterpret_cast<unsigned long long*>(dev_out), c->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_stage_sort(xnyz_ctx* c, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits) {
+    if (!c || !dev_keys || key_bits < 0 || key_bits > 64) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    if (n >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 keys");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int passes = static_cast<int>(cdiv(key_bits, 8));
+    if (passes == 0 || n <= 1) return XNYZ_OK;
+    Plan pl;
+    const size_t ok = pl.add(8 * n), ov = pl.add(4 * n);
+    TRY(ensure_arena(c, pl.total));
+    SortBufs sb{{reinterpret_cast<unsigned long long*>(dev_keys), at<unsigned long long>(c, ok)},
+                {dev_payload, dev_payload ? at<uint32_t>(c, ov) : nullptr}};
+    TRY(memset_small(c, offsetof(Small, sort_hist), sizeof(uint32_t) * 8 * 256, 0));
+    TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
+    launch_sort_histogram(sb.keys[0], n, passes, c->d_small->sort_hist, c->stream);
+    int res = 0;
+    TRY(radix_sort(c, sb, n, passes, c->d_small->sort_hist, res));
+    if (res) {
+        CUDA_TRY(cudaMemcpyAsync(dev_keys, sb.keys[1], 8 * n, cudaMemcpyDeviceToDevice, c->stream));
+        if (dev_payload) CUDA_TRY(cudaMemcpyAsync(dev_payload, sb.vals[1], 4 * n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return check_device_errors(c);
+}
+
+xnyz_status xnyz_host_hilbert(const uint64_t* in, uint64_t n, unsigned iteration, int inverse, uint64_t* out) {
+    if ((!in || !out) && n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (iteration > 20) return fail(XNYZ_ERR_UNSUPPORTED, "iteration above 20");
+    const auto& hm = hilbert_machines();
+    for (uint64_t i = 0; i < n; ++i)
+        out[i] = hilbert_apply_host(inverse ? hm.inv : hm.fwd, in[i], static_cast<int>(iteration), 0u);
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_host_codebook(int symtype, int count_stream, const uint64_t* symbols, const uint64_t* counts,
+                               const uint64_t* first_index, uint64_t nsyms, uint64_t total, uint8_t* meta,
+                               uint64_t* meta_len, uint64_t* encoded_bits, int* exp_golomb) {
+    if ((nsyms && (!symbols || !counts || !first_index)) || !meta_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    std::vector<SymbolStat> st(nsyms);
+    for (uint64_t i = 0; i < nsyms; ++i) st[i] = SymbolStat{symbols[i], counts[i], first_index[i]};
+    const SymType t = symtype == 0 ? SymType::U64 : (symtype == 1 ? SymType::U8 : SymType::I32);
+    const StreamCode sc = count_stream ? build_count_code(st, total) : build_stream_code(t, st, total);
+    const uint64_t cap = *meta_len;
+    *meta_len = sc.meta.size();
+    if (meta && cap) std::memcpy(meta, sc.meta.data(), std::min<uint64_t>(cap, sc.meta.size()));
+    if (encoded_bits) *encoded_bits = sc.encoded_bits;
+    if (exp_golomb) *exp_golomb = sc.exp_golomb;
+    return XNYZ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,534 @@
+// Compress-side stream kernels over the sorted keys.
+//
+//   units_*       one pass over the sorted keys: RLE run heads (unique cells), block heads,
+//                 quad / repos deltas (block mode) or SFC deltas (direct mode), PFor symbols
+//                 and patches, symbol histograms with first-occurrence units, all placed by
+//                 a three-channel chained scan (units, patches, blocks).
+//   count_stats   -rle count per unit and its histogram.
+//   block_deltas  + bitpack: BitPacker<uint64_t> of the block-id and block-count deltas.
+//   gr_encode     GolombRiceCoder<uint64_t>::pack of the patches.
+//   huff_encode_* HuffmanEncoder<T>::encode / exp-Golomb encode with host-built codes.
+//
+// Reference (paths relative to its source/): quantizer/block_quantizer.hpp:117-149 (LCP
+// streams), composer/block_compressor.hpp:110-114,146-147 (deltas), encoder/
+// p_for_delta_encoder.hpp:27-43 (PFor, limit 254), encoder/golomb_rice_encoder.hpp:92-148,
+// encoder/bitpacking_encoder.hpp:17-51, encoder/huffman_encoder.hpp:150-170,365-396,
+// composer/block_compressor_rle.hpp:97-123,290-308 (dedup and count stream).
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace xnyz {
+namespace dev {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;
+static_assert(kTile == kUnitTile && kTile == kEncTile, "tile size");
+
+__device__ __forceinline__ void block_key_fields(u64 k, const BlockKeyParams& kp, u64& id, u32& quad, u32& sfc) {
+    id = (kp.defect_flag && k >= kp.defect_flag) ? (((k - kp.defect_flag) >> 21) + kp.defect_base) : (k >> 21);
+    quad = (u32)(k >> 18) & 7u;
+    sfc = (u32)(k & 0x3ffffu);
+}
+
+__device__ __forceinline__ u64 direct_key_sfc(u64 k, const DirectKeyParams& kp) {
+    return (kp.defect_flag && k >= kp.defect_flag) ? (kp.defect_high | (k - kp.defect_flag)) : k;
+}
+
+// Warp-aggregated histogram update with first-occurrence tracking; the lowest lane of a
+// group of equal symbols holds the smallest unit index (units grow with the lane).
+__device__ __forceinline__ void hist_add(u32* hist, u32* first, bool valid, u32 sym, u32 unit) {
+    const u32 peers = __match_any_sync(kFullMask, valid ? sym : (0x10000u | lane_id()));
+    if (valid && lane_id() == (u32)(__ffs(peers) - 1)) {
+        atomicAdd(&hist[sym], (u32)__popc(peers));
+        atomicMin(&first[sym], unit);
+    }
+}
+
+template <bool DIRECT>
+__global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__ keys, u64 n, int rle,
+                                                         BlockKeyParams bkp, DirectKeyParams dkp, UnitOutputs out,
+                                                         LookBackState lb, u32* tile_counter, u32* err) {
+    __shared__ u64 sk[kTile + 1];
+    __shared__ u64 scratch[16];
+    __shared__ u32 slot;
+    __shared__ u64 sbase[3];
+    __shared__ u32 hrep[256], frep[256], hquad[16], fquad[16];
+    __shared__ u64 psum[kThreads / 32];
+
+    const u32 tile = claim_tile(tile_counter, &slot);
+    const u32 ntiles = gridDim.x;
+    const u64 base = (u64)tile * kTile;
+    const u32 cnt = (u32)min((u64)kTile, n - base);
+    const int tid = threadIdx.x;
+    if (tid == 0) sk[0] = base ? keys[base - 1] : 0ull;
+    for (int i = 0; i < kItems; ++i) {
+        const u32 e = (u32)i * kThreads + tid;
+        if (e < cnt) sk[1 + e] = keys[base + e];
+    }
+    hrep[tid] = 0;
+    frep[tid] = 0xffffffffu;
+    if (tid < 16) {
+        hquad[tid] = 0;
+        fquad[tid] = 0xffffffffu;
+    }
+    __syncthreads();
+
+    // Pass A: classify my 16 consecutive elements.
+    u64 val[kItems];  // repos / sfc delta
+    u64 idv[kItems];  // block id (block mode)
+    u32 fl[kItems];   // bit0 head, bit1 patch, bit2 new block, bits 8..15 quad delta
+    u32 h = 0, p = 0, b = 0;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const u32 e = (u32)tid * kItems + i;
+        fl[i] = 0;
+        val[i] = 0;
+        idv[i] = 0;
+        if (e >= cnt) continue;
+        const u64 j = base + e;
+        const u64 k = sk[1 + e], kp = sk[e];
+        const bool head = !rle || j == 0 || k != kp;
+        if (!head) continue;
+        u32 f = 1u;
+        if (DIRECT) {
+            const u64 s = direct_key_sfc(k, dkp);
+            const u64 d = j == 0 ? s : s - direct_key_sfc(kp, dkp);
+            val[i] = d;
+            if (d > 254u) f |= 2u;
+        } else {
+            u64 id, idp = 0;
+            u32 quad, sfc, quadp = 0, sfcp = 0;
+            block_key_fields(k, bkp, id, quad, sfc);
+            if (j > 0) block_key_fields(kp, bkp, idp, quadp, sfcp);
+            const bool nb = (j == 0) || id != idp;
+            u32 qd;
+            u64 r;
+            if (nb) {
+                qd = quad;
+                r = sfc;
+                f |= 4u;
+            } else if (quad != quadp) {
+                qd = quad - quadp;
+                r = sfc;
+            } else {
+                qd = 0;
+                r = (u64)sfc - (u64)sfcp;
+            }
+            val[i] = r;
+            idv[i] = id;
+            if (r > 254u) f |= 2u;
+            f |= (qd & 0xffu) << 8;
+        }
+        fl[i] = f;
+        h += 1;
+        p += (f >> 1) & 1u;
+        b += (f >> 2) & 1u;
+    }
+    // Packed three-field exclusive scan: each field <= 4096 per tile, 21 bits apiece.
+    const u64 mine = (u64)h | ((u64)p << 21) | ((u64)b << 42);
+    u64 tot;
+    const u64 ex = block_exclusive<kThreads>(mine, 0ull, AddOp{}, scratch, tot);
+    if (tid == 0 || tid == 32 || tid == 64) {
+        const int ch = tid >> 5;
+        const u64 part = (tot >> (21 * ch)) & ((1ull << 21) - 1);
+        LookBack64 l{lb.flag + ch * ntiles, lb.agg + ch * ntiles, lb.inc + ch * ntiles};
+        const u64 before = lookback_add(l, tile, part, err);
+        sbase[ch] = before;
+        if (tile == ntiles - 1) out.counters[ch] = before + part;
+    }
+    __syncthreads();
+
+    u64 uu = sbase[0] + (ex & ((1ull << 21) - 1));
+    u64 pp = sbase[1] + ((ex >> 21) & ((1ull << 21) - 1));
+    u64 bb = sbase[2] + ((ex >> 42) & ((1ull << 21) - 1));
+    u64 mysum = 0;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const u32 f = fl[i];
+        const bool head = f & 1u;
+        const bool patch = (f >> 1) & 1u;
+        const u32 sym = head ? (patch ? 0u : (u32)val[i] + 1u) : 0u;
+        const u32 qsym = ((f >> 8) & 0xffu) + 1u;
+        if (head) {
+            out.rep_sym[uu] = (u8)sym;
+            if (!DIRECT) out.quad_sym[uu] = (u8)qsym;
+            if (patch) {
+                out.patches[pp] = val[i];
+                mysum += val[i];
+            }
+            if (!DIRECT && ((f >> 2) & 1u)) {
+                out.blk_id[bb] = idv[i];
+                out.blk_unit[bb] = (u32)uu;
+            }
+            if (rle) out.unit_pos[uu] = (u32)(base + (u32)tid * kItems + i);
+        }
+        hist_add(hrep, frep, head, sym, (u32)uu);
+        if (!DIRECT) hist_add(hquad, fquad, head, qsym, (u32)uu);
+        uu += head;
+        pp += head && patch;
+        bb += head && ((f >> 2) & 1u);
+    }
+    for (int d = 16; d > 0; d >>= 1) mysum += __shfl_xor_sync(kFullMask, mysum, d);
+    if (lane_id() == 0) psum[tid >> 5] = mysum;
+    __syncthreads();
+    if (tid == 0) {
+        u64 s = 0;
+        for (int w = 0; w < kThreads / 32; ++w) s += psum[w];
+        if (s) atomicAdd(&out.counters[3], s);
+    }
+    if (hrep[tid]) {
+        atomicAdd(&out.hist_rep[tid], (u64)hrep[tid]);
+        atomicMin(&out.first_rep[tid], frep[tid]);
+    }
+    if (!DIRECT && tid < 16 && hquad[tid]) {
+        atomicAdd(&out.hist_quad[tid], (u64)hquad[tid]);
+        atomicMin(&out.first_quad[tid], fquad[tid]);
+    }
+}
+
+// -rle: count of each unit = distance to the next unit's first point.
+__global__ void __launch_bounds__(kThreads) count_stats_kernel(const u32* __restrict__ unit_pos, u64 units, u64 n,
+                                                               i32* __restrict__ counts, CountStats cs) {
+    __shared__ u32 sh[kCountDense], sf[kCountDense];
+    for (int i = threadIdx.x; i < kCountDense; i += kThreads) {
+        sh[i] = 0;
+        sf[i] = 0xffffffffu;
+    }
+    __syncthreads();
+    const u64 stride = (u64)gridDim.x * kThreads;
+    const u64 start = (u64)blockIdx.x * kThreads + (threadIdx.x & ~31u);
+    for (u64 b0 = start; b0 < units; b0 += stride) {
+        const u64 u = b0 + lane_id();
+        const bool ok = u < units;
+        u32 c = 0;
+        if (ok) {
+            const u64 nxt = (u + 1 < units) ? (u64)unit_pos[u + 1] : n;
+            c = (u32)(nxt - unit_pos[u]);
+            counts[u] = (i32)c;
+        }
+        const bool dense = ok && c < (u32)kCountDense;
+        hist_add(sh, sf, dense, c, (u32)u);
+        if (ok && !dense) {
+            const u32 slot = atomicAdd(cs.over_n, 1u);
+            cs.over_val[slot] = c;
+            cs.over_unit[slot] = (u32)u;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kCountDense; i += kThreads)
+        if (sh[i]) {
+            atomicAdd(&cs.hist[i], (u64)sh[i]);
+            atomicMin(&cs.first[i], sf[i]);
+        }
+}
+
+__global__ void __launch_bounds__(kThreads) block_deltas_kernel(const u64* __restrict__ blk_id,
+                                                                const u32* __restrict__ blk_unit, u64 nb, u64 units,
+                                                                u64* __restrict__ d_blk, u64* __restrict__ d_cnt,
+                                                                u64* max2) {
+    __shared__ u64 s0[kThreads / 32], s1[kThreads / 32];
+    u64 m0 = 0, m1 = 0;
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 b = (u64)blockIdx.x * kThreads + threadIdx.x; b < nb; b += stride) {
+        const u64 cb = ((b + 1 < nb) ? (u64)blk_unit[b + 1] : units) - blk_unit[b];
+        u64 db, dc;
+        if (b == 0) {
+            db = blk_id[0];
+            dc = cb;
+        } else {
+            const u64 cp = (u64)blk_unit[b] - blk_unit[b - 1];
+            db = blk_id[b] - blk_id[b - 1];
+            dc = cb - cp;  // wraps like the reference's in-place u64 differences
+        }
+        d_blk[b] = db;
+        d_cnt[b] = dc;
+        m0 = max(m0, db);
+        m1 = max(m1, dc);
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        m0 = max(m0, __shfl_xor_sync(kFullMask, m0, d));
+        m1 = max(m1, __shfl_xor_sync(kFullMask, m1, d));
+    }
+    if (lane_id() == 0) {
+        s0[threadIdx.x >> 5] = m0;
+        s1[threadIdx.x >> 5] = m1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kThreads / 32; ++w) {
+            m0 = max(m0, s0[w]);
+            m1 = max(m1, s1[w]);
+        }
+        m0 = max(m0, s0[0]);
+        m1 = max(m1, s1[0]);
+        atomicMax(&max2[0], m0);
+        atomicMax(&max2[1], m1);
+    }
+}
+
+// BitPacker: value b at bit b*width, LSB-first.
+__global__ void __launch_bounds__(kThreads) bitpack_kernel(const u64* __restrict__ vals, u64 n, int width,
+                                                           u32* words) {
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 b0 = (u64)blockIdx.x * kThreads + (threadIdx.x & ~31u); b0 < n; b0 += stride) {
+        const u64 b = b0 + lane_id();
+        const bool ok = b < n;
+        warp_write_lsb(words, b * (u64)width, ok ? vals[b] : 0ull, ok ? (u32)width : 0u);
+    }
+}
+
+// Shared skeleton of the chained-scan encoders: stage a tile of inputs, give every element
+// its bit length, scan, look back, write.
+template <typename T>
+__device__ __forceinline__ u32 stage_tile(const T* __restrict__ in, u64 n, T* s, u32* slot, u32* tile_counter,
+                                          u32& tile, u64& base) {
+    tile = claim_tile(tile_counter, slot);
+    base = (u64)tile * kTile;
+    const u32 cnt = (u32)min((u64)kTile, n - base);
+    for (int i = 0; i < kItems; ++i) {
+        const u32 e = (u32)i * kThreads + threadIdx.x;
+        if (e < cnt) s[e] = in[base + e];
+    }
+    __syncthreads();
+    return cnt;
+}
+
+__device__ __forceinline__ u64 tile_bit_base(LookBackState lb, u32 tile, u64 tot, u64* sbase,
+                                             unsigned long long* total_bits, u32* err) {
+    if (threadIdx.x == 0) {
+        LookBack64 l{lb.flag, lb.agg, lb.inc};
+        const u64 before = lookback_add(l, tile, tot, err);
+        *sbase = before;
+        if (tile == gridDim.x - 1) *total_bits = before + tot;
+    }
+    __syncthreads();
+    return *sbase;
+}
+
+__global__ void __launch_bounds__(kThreads) gr_encode_kernel(const u64* __restrict__ vals, u64 n, int k, u32* words,
+                                                             u64 cap_bits, LookBackState lb, u32* tile_counter,
+                                                             unsigned long long* total_bits, u32* err) {
+    __shared__ u64 sv[kTile];
+    __shared__ u64 scratch[16];
+    __shared__ u32 slot;
+    __shared__ u64 sbase;
+    u32 tile;
+    u64 base;
+    const u32 cnt = stage_tile(vals, n, sv, &slot, tile_counter, tile, base);
+    const u32 e0 = threadIdx.x * kItems;
+    u64 sum = 0;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+        if (e0 + i < cnt) sum += (sv[e0 + i] >> k) + 1u + (u64)k;
+    u64 tot;
+    const u64 ex = block_exclusive<kThreads>(sum, 0ull, AddOp{}, scratch, tot);
+    u64 pos = tile_bit_base(lb, tile, tot, &sbase, total_bits, err) + ex;
+    const u64 mask = k ? ((1ull << k) - 1) : 0ull;
+#pragma unroll 1
+    for (int i = 0; i < kItems; ++i) {
+        const bool ok = e0 + i < cnt;
+        const u64 v = ok ? sv[e0 + i] : 0ull;
+        const u64 q = v >> k;
+        u64 wval = 0, wpos = pos;
+        u32 nb = 0;
+        if (ok && pos + q + 1u + (u64)k > cap_bits) {  // output bound (never reached with valid sizes)
+            atomicOr(err, kErrOverflow);
+        } else if (ok) {
+            if (q + 1u + (u64)k <= 64u) {
+                wval = ((q ? ((1ull << q) - 1) : 0ull)) | ((v & mask) << (q + 1));
+                nb = (u32)(q + 1 + k);
+            } else {
+                write_ones_lsb(words, pos, q);  // long unary run, written by this lane alone
+                wval = (v & mask) << 1;
+                nb = 1u + (u32)k;
+                wpos = pos + q;
+            }
+        }
+        warp_write_lsb(words, wpos, wval, nb);
+        if (ok) pos += q + 1u + (u64)k;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) huff_encode_u8_kernel(const u8* __restrict__ sym, u64 n,
+                                                                  const ByteCodes* __restrict__ codes, u32* words,
+                                                                  u64 cap_bits, LookBackState lb, u32* tile_counter,
+                                                                  unsigned long long* total_bits, u32* err) {
+    __shared__ u8 ss[kTile];
+    __shared__ u32 cbits[256];
+    __shared__ u8 clen[256];
+    __shared__ u64 scratch[16];
+    __shared__ u32 slot;
+    __shared__ u64 sbase;
+    cbits[threadIdx.x] = codes->bits[threadIdx.x];
+    clen[threadIdx.x] = codes->len[threadIdx.x];
+    u32 tile;
+    u64 base;
+    const u32 cnt = stage_tile(sym, n, ss, &slot, tile_counter, tile, base);
+    const u32 e0 = threadIdx.x * kItems;
+    u64 sum = 0;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+        if (e0 + i < cnt) sum += clen[ss[e0 + i]];
+    u64 tot;
+    const u64 ex = block_exclusive<kThreads>(sum, 0ull, AddOp{}, scratch, tot);
+    u64 pos = tile_bit_base(lb, tile, tot, &sbase, total_bits, err) + ex;
+#pragma unroll 4
+    for (int i = 0; i < kItems; ++i) {
+        const bool ok = e0 + i < cnt;
+        const u32 s = ok ? ss[e0 + i] : 0u;
+        u32 len = ok ? clen[s] : 0u;
+        if (pos + len > cap_bits) {  // output bound (never reached with valid sizes)
+            if (len) atomicOr(err, kErrOverflow);
+            len = 0;
+        }
+        // Codes longer than 32 bits are the 32-bit value zero-extended (huffman_encoder.hpp:251).
+        const u32 nb = len > 32u ? 32u : len;
+        warp_write_msb(words, pos + (len - nb), cbits[s], nb);
+        pos += len;
+    }
+}
+
+__device__ __forceinline__ u32 rev_low(u64 v, int k) { return k ? (__brev((u32)v) >> (32 - k)) : 0u; }
+
+__global__ void __launch_bounds__(kThreads) count_encode_kernel(const i32* __restrict__ counts, u64 n, int eg_k,
+                                                                const u32* __restrict__ dense_bits,
+                                                                const u8* __restrict__ dense_len,
+                                                                const u32* __restrict__ sparse_val,
+                                                                const u32* __restrict__ sparse_bits,
+                                                                const u8* __restrict__ sparse_len, u32 sparse_n,
+                                                                u32* words, u64 cap_bits, LookBackState lb,
+                                                                u32* tile_counter,
+                                                                unsigned long long* total_bits, u32* err) {
+    __shared__ i32 sc[kTile];
+    __shared__ u64 scratch[16];
+    __shared__ u32 slot;
+    __shared__ u64 sbase;
+    u32 tile;
+    u64 base;
+    const u32 cnt = stage_tile(counts, n, sc, &slot, tile_counter, tile, base);
+    const u32 e0 = threadIdx.x * kItems;
+    // code of one count: (length, value bits, bit offset of the value inside the code)
+    auto code = [&](i32 c, u32& len, u64& val, u32& nb) {
+        if (eg_k >= 0) {
+            const long long s = c;
+            const u64 z = ((u64)s << 1) ^ (u64)(s >> 63);
+            const u64 n1 = (z >> eg_k) + 1u;
+            const u32 lz = bitlen64(n1) - 1u;
+            len = 2u * lz + 1u + (u32)eg_k;
+            nb = lz + 1u + (u32)eg_k;
+            val = (n1 << eg_k) | rev_low(z, eg_k);
+        } else {
+            const u32 uc = (u32)c;
+            u32 bits = 0, l = 0;
+            if (uc < (u32)kCountDense) {
+                bits = dense_bits[uc];
+                l = dense_len[uc];
+            } else {
+                u32 lo = 0, hi = sparse_n;
+                while (lo < hi) {
+                    const u32 mid = (lo + hi) >> 1;
+                    if (sparse_val[mid] < uc) lo = mid + 1; else hi = mid;
+                }
+                if (lo < sparse_n && sparse_val[lo] == uc) {
+                    bits = sparse_bits[lo];
+                    l = sparse_len[lo];
+                } else {
+                    atomicOr(err, kErrOverflow);
+                }
+            }
+            len = l;
+            nb = l > 32u ? 32u : l;
+            val = bits;
+        }
+    };
+    u64 sum = 0;
+    for (int i = 0; i < kItems; ++i)
+        if (e0 + i < cnt) {
+            u32 len, nb;
+            u64 val;
+            code(sc[e0 + i], len, val, nb);
+            sum += len;
+        }
+    u64 tot;
+    const u64 ex = block_exclusive<kThreads>(sum, 0ull, AddOp{}, scratch, tot);
+    u64 pos = tile_bit_base(lb, tile, tot, &sbase, total_bits, err) + ex;
+    for (int i = 0; i < kItems; ++i) {
+        const bool ok = e0 + i < cnt;
+        u32 len = 0, nb = 0;
+        u64 val = 0;
+        if (ok) code(sc[e0 + i], len, val, nb);
+        if (pos + len > cap_bits) {  // output bound (never reached with valid sizes)
+            if (len) atomicOr(err, kErrOverflow);
+            len = 0;
+            nb = 0;
+        }
+        warp_write_msb(words, pos + (len - nb), val, nb);
+        pos += len;
+    }
+}
+
+inline int persistent_grid(u64 n) {
+    u64 want = (n + kThreads - 1) / kThreads;
+    if (want < 1) want = 1;
+    return (int)(want < 148ull * 8ull ? want : 148ull * 8ull);
+}
+
+}  // namespace
+
+void launch_units_block(const unsigned long long* keys, uint64_t n, int rle, BlockKeyParams kp, UnitOutputs out,
+                        LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
+    if (!tiles) return;
+    units_kernel<false><<<tiles, kThreads, 0, st>>>(keys, n, rle, kp, DirectKeyParams{}, out, lb, tile_counter, err);
+}
+void launch_units_direct(const unsigned long long* keys, uint64_t n, int rle, DirectKeyParams kp, UnitOutputs out,
+                         LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
+    if (!tiles) return;
+    units_kernel<true><<<tiles, kThreads, 0, st>>>(keys, n, rle, BlockKeyParams{}, kp, out, lb, tile_counter, err);
+}
+void launch_count_stats(const uint32_t* unit_pos, uint64_t units, uint64_t n, int32_t* counts, CountStats cs,
+                        cudaStream_t st) {
+    count_stats_kernel<<<persistent_grid(units), kThreads, 0, st>>>(unit_pos, units, n, counts, cs);
+}
+void launch_block_deltas(const unsigned long long* blk_id, const uint32_t* blk_unit, uint64_t nblocks, uint64_t units,
+                         unsigned long long* d_blk, unsigned long long* d_cnt, unsigned long long* max2,
+                         cudaStream_t st) {
+    block_deltas_kernel<<<persistent_grid(nblocks), kThreads, 0, st>>>(blk_id, blk_unit, nblocks, units, d_blk, d_cnt,
+                                                                       max2);
+}
+void launch_bitpack(const unsigned long long* vals, uint64_t n, int width, uint32_t* words, cudaStream_t st) {
+    bitpack_kernel<<<persistent_grid(n), kThreads, 0, st>>>(vals, n, width, words);
+}
+void launch_gr_encode(const unsigned long long* vals, uint64_t n, int k, uint32_t* words, uint64_t cap_bits,
+                      LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits, uint32_t* err,
+                      cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
+    if (!tiles) return;
+    gr_encode_kernel<<<tiles, kThreads, 0, st>>>(vals, n, k, words, cap_bits, lb, tile_counter, total_bits, err);
+}
+void launch_huff_encode_u8(const uint8_t* sym, uint64_t n, const ByteCodes* codes, uint32_t* words,
+                           uint64_t cap_bits, LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits,
+                           uint32_t* err, cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
+    if (!tiles) return;
+    huff_encode_u8_kernel<<<tiles, kThreads, 0, st>>>(sym, n, codes, words, cap_bits, lb, tile_counter, total_bits,
+                                                      err);
+}
+void launch_count_encode(const int32_t* counts, uint64_t n, int eg_k, const uint32_t* dense_bits,
+                         const uint8_t* dense_len, const uint32_t* sparse_val, const uint32_t* sparse_bits,
+                         const uint8_t* sparse_len, uint32_t sparse_n, uint32_t* words, uint64_t cap_bits,
+                         LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits, uint32_t* err,
+                         cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
+    if (!tiles) return;
+    count_encode_kernel<<<tiles, kThreads, 0, st>>>(counts, n, eg_k, dense_bits, dense_len, sparse_val, sparse_bits,
+                                                    sparse_len, sparse_n, words, cap_bits, lb, tile_counter,
+                                                    total_bits, err);
+}
+
+}  // namespace dev
+}  // namespace xnyz

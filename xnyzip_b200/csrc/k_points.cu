@@ -1,0 +1,341 @@
+// Point-level kernels: bounding-box minimum (shift_points), quantization with range and
+// error statistics, and sort-key generation for block and direct mode.
+//
+// Reference behaviour restated here (paths relative to the reference's source/):
+//   shift_points           preprocessor/shifting.hpp:11-36  (strict '<' scan from FLT_MAX)
+//   quantize               quantizer/truncated_octahedron_quantizer.hpp:21-55, cube_quantizer.hpp:15-27
+//   ranges / direct switch composer/block_compressor.hpp:69-88
+//   error statistics       composer/block_compressor_rle.hpp:53-67
+//   block keys             quantizer/block_quantizer.hpp:93-115
+//   direct keys            composer/block_compressor.hpp:90-101
+#include <cfloat>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace xnyz {
+namespace dev {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Order key of a float for the minimum scan: monotone in value, +0 and -0 equal, NaN last.
+__device__ __forceinline__ u32 order_key(float f) {
+    u32 b = __float_as_uint(f);
+    if ((b & 0x7fffffffu) > 0x7f800000u) return 0xffffffffu;  // NaN never wins ('<' is false)
+    if ((b & 0x7fffffffu) == 0u) b = 0u;                        // -0 ties with +0
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) { return a < b ? a : b; }
+
+// Minimum over the block of three u64 values, then one atomicMin per axis.
+__device__ void block_min3(unsigned long long m[3], unsigned long long* dst) {
+    __shared__ unsigned long long sm[3][kThreads / 32];
+    for (int a = 0; a < 3; ++a) {
+        unsigned long long v = m[a];
+        for (int d = 16; d > 0; d >>= 1) v = umin64(v, __shfl_xor_sync(kFullMask, v, d));
+        if (lane_id() == 0) sm[a][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        unsigned long long v = sm[threadIdx.x][0];
+        for (int w = 1; w < kThreads / 32; ++w) v = umin64(v, sm[threadIdx.x][w]);
+        atomicMin(&dst[threadIdx.x], v);
+    }
+}
+
+// shift_points keeps the first of equal minima; the key packs (order key, index) so the
+// smallest index wins ties (including +0 / -0), and the initial FLT_MAX candidate carries
+// index 0xffffffff.
+__global__ void __launch_bounds__(kThreads) bbox_kernel(const float* __restrict__ xyz, u64 n, PointStats* stats) {
+    unsigned long long m[3];
+    for (int a = 0; a < 3; ++a) m[a] = ~0ull;
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const float* p = xyz + 3 * i;
+        for (int a = 0; a < 3; ++a) {
+            unsigned long long k = ((unsigned long long)order_key(__ldg(p + a)) << 32) | (u32)i;
+            m[a] = umin64(m[a], k);
+        }
+    }
+    block_min3(m, stats->minkey);
+}
+
+__device__ __forceinline__ void load_offset(const float* xyz, const PointStats* st, float off[3]) {
+    for (int a = 0; a < 3; ++a) {
+        const unsigned long long k = st->minkey[a];
+        const u32 idx = (u32)(k & 0xffffffffu);
+        const u32 ok = (u32)(k >> 32);
+        // The reference starts from FLT_MAX; a candidate wins only if strictly smaller.
+        off[a] = (idx == 0xffffffffu || ok >= order_key(FLT_MAX)) ? FLT_MAX : xyz[3 * (u64)idx + a];
+    }
+}
+
+__device__ __forceinline__ bool finite3(float x, float y, float z) {
+    return isfinite(x) && isfinite(y) && isfinite(z);
+}
+
+__global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* __restrict__ xyz, u64 n,
+                                                                  QuantParams q, PointStats* stats,
+                                                                  int with_error_stats) {
+    __shared__ float off[3];
+    __shared__ int smax[3][kThreads / 32], smin[3][kThreads / 32];
+    __shared__ u32 snf[kThreads / 32], smse[kThreads / 32];
+    __shared__ double ssum[kThreads / 32];
+    if (threadIdx.x == 0) {
+        load_offset(xyz, stats, off);
+        if (blockIdx.x == 0)
+            for (int a = 0; a < 3; ++a) stats->offset[a] = off[a];
+    }
+    __syncthreads();
+    const float ox = off[0], oy = off[1], oz = off[2];
+    int mx[3] = {0, 0, 0};
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX};
+    u32 nonfinite = 0;
+    float emax = 0.0f;
+    double esum = 0.0;
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const float x = __ldg(xyz + 3 * i), y = __ldg(xyz + 3 * i + 1), z = __ldg(xyz + 3 * i + 2);
+        if (!finite3(x, y, z)) {
+            ++nonfinite;
+            continue;
+        }
+        const float px = __fsub_rn(x, ox), py = __fsub_rn(y, oy), pz = __fsub_rn(z, oz);
+        i32 c[3];
+        quantize(q, px, py, pz, c[0], c[1], c[2]);
+        for (int a = 0; a < 3; ++a) {
+            mx[a] = max(mx[a], c[a]);
+            mn[a] = min(mn[a], c[a]);
+        }
+        if (with_error_stats) {
+            // (sx - rx)^2 + (sy - ry)^2 + (sz - rz)^2 in float, left to right.
+            float rx, ry, rz;
+            recover(q, c[0], c[1], c[2], 0.0f, 0.0f, 0.0f, rx, ry, rz);
+            const float dx = __fsub_rn(px, rx), dy = __fsub_rn(py, ry), dz = __fsub_rn(pz, rz);
+            const float e = __fadd_rn(__fadd_rn(sqf(dx), sqf(dy)), sqf(dz));
+            emax = fmaxf(emax, e);
+            esum += (double)e;
+        }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        for (int a = 0; a < 3; ++a) {
+            mx[a] = max(mx[a], __shfl_xor_sync(kFullMask, mx[a], d));
+            mn[a] = min(mn[a], __shfl_xor_sync(kFullMask, mn[a], d));
+        }
+        nonfinite += __shfl_xor_sync(kFullMask, nonfinite, d);
+        emax = fmaxf(emax, __shfl_xor_sync(kFullMask, emax, d));
+        esum += __shfl_xor_sync(kFullMask, esum, d);
+    }
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0) {
+        for (int a = 0; a < 3; ++a) {
+            smax[a][w] = mx[a];
+            smin[a][w] = mn[a];
+        }
+        snf[w] = nonfinite;
+        smse[w] = __float_as_uint(emax);
+        ssum[w] = esum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int bx[3] = {0, 0, 0}, bn[3] = {INT_MAX, INT_MAX, INT_MAX};
+        u32 nf = 0, em = 0;
+        double es = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) {
+            for (int a = 0; a < 3; ++a) {
+                bx[a] = max(bx[a], smax[a][k]);
+                bn[a] = min(bn[a], smin[a][k]);
+            }
+            nf += snf[k];
+            em = max(em, smse[k]);
+            es += ssum[k];
+        }
+        for (int a = 0; a < 3; ++a) {
+            atomicMax(&stats->max_cell[a], bx[a]);
+            atomicMin(&stats->min_cell[a], bn[a]);
+        }
+        if (nf) atomicAdd(&stats->nonfinite, nf);
+        if (with_error_stats) {
+            atomicMax(&stats->mse_max_bits, em);
+            atomicAdd(&stats->mse_sum, es);
+        }
+    }
+}
+
+// Per-block histograms of the sort digits, flushed with one atomicAdd per non-zero bin.
+struct DigitHist {
+    u32* s;  // shared [passes * 256]
+    int passes;
+    __device__ __forceinline__ void add(u64 key) {
+        for (int p = 0; p < passes; ++p) atomicAdd(&s[p * 256 + (u32)((key >> (8 * p)) & 255u)], 1u);
+    }
+};
+
+__device__ __forceinline__ void stage_hilbert_table(const u8* g, u8* s) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) s[i] = g ? g[i] : 0;
+}
+
+// Block mode: key = id << 21 | quad << 18 | sfc18 with the reference's size_t arithmetic
+// (negative lattice indices wrap to 2^64 + v before the division by 64).
+__device__ __forceinline__ u64 block_key(i32 x, i32 y, i32 z, const BlockKeyParams& kp, const u8* htab) {
+    const u64 X = (u64)(i64)x, Y = (u64)(i64)y, Z = (u64)(i64)z;
+    const u64 cx = X >> 6, cy = Y >> 6, cz = Z >> 6;
+    const u32 dx = (u32)(X & 63u), dy = (u32)(Y & 63u), dz = (u32)(Z & 63u);
+    u64 m = morton3((i32)dx, (i32)dy, (i32)dz);
+    if (kp.hilbert) m = hilbert_apply(htab, m, 5, kp.hstart);
+    const u64 quad = (cx & 1u) | ((cy & 1u) << 1) | ((cz & 1u) << 2);
+    const u64 low = (quad << 18) | m;
+    const u64 xy = (cx >> 1) + (cy >> 1) * kp.nx;
+    if (z >= 0) return ((xy + (cz >> 1) * kp.nx * kp.ny) << 21) | low;
+    return kp.defect_flag | (xy << 21) | low;  // z == -1: id = xy + defect_base
+}
+
+__global__ void __launch_bounds__(kThreads) keys_block_kernel(const float* __restrict__ xyz, u64 n, QuantParams q,
+                                                              const PointStats* stats, BlockKeyParams kp,
+                                                              const u8* __restrict__ htab_g,
+                                                              unsigned long long* __restrict__ keys,
+                                                              u32* __restrict__ payload, int passes, u32* hist) {
+    __shared__ float off[3];
+    __shared__ u8 htab[256];
+    __shared__ u32 sh[8 * 256];
+    if (threadIdx.x == 0) load_offset(xyz, stats, off);
+    stage_hilbert_table(htab_g, htab);
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    DigitHist dh{sh, passes};
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const float px = __fsub_rn(__ldg(xyz + 3 * i), off[0]);
+        const float py = __fsub_rn(__ldg(xyz + 3 * i + 1), off[1]);
+        const float pz = __fsub_rn(__ldg(xyz + 3 * i + 2), off[2]);
+        i32 x, y, z;
+        quantize(q, px, py, pz, x, y, z);
+        const u64 k = block_key(x, y, z, kp, htab);
+        keys[i] = k;
+        if (payload) payload[i] = (u32)i;
+        if (passes) dh.add(k);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// Direct mode: key = global Morton or Hilbert code (hilbert_bits levels); z == -1 cells keep
+// their transformed low levels under defect_flag.
+__global__ void __launch_bounds__(kThreads) keys_direct_kernel(const float* __restrict__ xyz, u64 n, QuantParams q,
+                                                               const PointStats* stats, DirectKeyParams kp,
+                                                               const u8* __restrict__ htab_g,
+                                                               unsigned long long* __restrict__ keys,
+                                                               u32* __restrict__ payload, int passes, u32* hist) {
+    __shared__ float off[3];
+    __shared__ u8 htab[256];
+    __shared__ u32 sh[8 * 256];
+    if (threadIdx.x == 0) load_offset(xyz, stats, off);
+    stage_hilbert_table(htab_g, htab);
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    DigitHist dh{sh, passes};
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const float px = __fsub_rn(__ldg(xyz + 3 * i), off[0]);
+        const float py = __fsub_rn(__ldg(xyz + 3 * i + 1), off[1]);
+        const float pz = __fsub_rn(__ldg(xyz + 3 * i + 2), off[2]);
+        i32 x, y, z;
+        quantize(q, px, py, pz, x, y, z);
+        u64 m = morton3(x, y, z);
+        if (kp.hilbert) m = hilbert_apply(htab, m, kp.bits, 0u);
+        const u64 k = (z >= 0) ? m : (kp.defect_flag | (m & (kp.defect_flag - 1)));
+        keys[i] = k;
+        if (payload) payload[i] = (u32)i;
+        if (passes) dh.add(k);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+__global__ void __launch_bounds__(kThreads) quantize_cells_kernel(const float* __restrict__ xyz, u64 n, QuantParams q,
+                                                                  const PointStats* stats, i32* __restrict__ cells) {
+    __shared__ float off[3];
+    if (threadIdx.x == 0) load_offset(xyz, stats, off);
+    __syncthreads();
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const float px = __fsub_rn(xyz[3 * i], off[0]);
+        const float py = __fsub_rn(xyz[3 * i + 1], off[1]);
+        const float pz = __fsub_rn(xyz[3 * i + 2], off[2]);
+        quantize(q, px, py, pz, cells[3 * i], cells[3 * i + 1], cells[3 * i + 2]);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) recover_cells_kernel(const i32* __restrict__ cells, u64 n, QuantParams q,
+                                                                 const float* __restrict__ off,
+                                                                 float* __restrict__ xyz) {
+    const u64 stride = (u64)gridDim.x * kThreads;
+    const float ox = off[0], oy = off[1], oz = off[2];
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        float x, y, z;
+        recover(q, cells[3 * i], cells[3 * i + 1], cells[3 * i + 2], ox, oy, oz, x, y, z);
+        xyz[3 * i] = x;
+        xyz[3 * i + 1] = y;
+        xyz[3 * i + 2] = z;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) hilbert_kernel(const unsigned long long* __restrict__ in, u64 n,
+                                                           const u8* __restrict__ tab_g, int top, u32 state,
+                                                           unsigned long long* __restrict__ out) {
+    __shared__ u8 tab[256];
+    stage_hilbert_table(tab_g, tab);
+    __syncthreads();
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) out[i] = hilbert_apply(tab, in[i], top, state);
+}
+
+int grid_for(u64 n) {
+    // Persistent-style grid: a few resident blocks per SM of the 148-SM B200.
+    u64 want = (n + kThreads - 1) / kThreads;
+    u64 cap = 148ull * 8ull;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+}  // namespace
+
+void launch_bbox(const float* xyz, uint64_t n, PointStats* stats, cudaStream_t st) {
+    bbox_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, stats);
+}
+void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
+                           cudaStream_t st) {
+    quantize_range_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, with_error_stats);
+}
+void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, BlockKeyParams kp,
+                       const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
+                       uint32_t* hist, cudaStream_t st) {
+    keys_block_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, kp, hilbert_tab, keys, payload, passes,
+                                                        hist);
+}
+void launch_keys_direct(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, DirectKeyParams kp,
+                        const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
+                        uint32_t* hist, cudaStream_t st) {
+    keys_direct_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, kp, hilbert_tab, keys, payload, passes,
+                                                         hist);
+}
+void launch_quantize_cells(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, int32_t* cells,
+                           cudaStream_t st) {
+    quantize_cells_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, cells);
+}
+void launch_recover_cells(const int32_t* cells, uint64_t n, QuantParams q, const float* offset3_dev, float* xyz,
+                          cudaStream_t st) {
+    recover_cells_kernel<<<grid_for(n), kThreads, 0, st>>>(cells, n, q, offset3_dev, xyz);
+}
+void launch_hilbert(const unsigned long long* in, uint64_t n, const uint8_t* tab, int top, unsigned int state,
+                    unsigned long long* out, cudaStream_t st) {
+    hilbert_kernel<<<grid_for(n), kThreads, 0, st>>>(in, n, tab, top, state, out);
+}
+
+}  // namespace dev
+}  // namespace xnyz

@@ -1,0 +1,226 @@
+// Launchers of the sm_100a kernels (implemented in k_*.cu), called by the host pipeline.
+// All pointers are device pointers unless named *_host; every launcher is asynchronous on
+// `st`.  Plain C++ types only, so host .cpp files include this without CUDA headers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+typedef struct CUstream_st* cudaStream_t;
+
+namespace xnyz {
+namespace dev {
+
+struct QuantParams {
+    int quantizer;  // 0 cube, 1 truncated octahedron
+    float div;      // float(double(2*l2)/sqrt(3|5))
+    float s;        // l2 as float
+    float rdiv;     // float(sqrt(3|5))
+};
+
+// Results of the bounding-box / quantization sweeps (one struct in device memory).
+struct PointStats {
+    unsigned long long minkey[3];  // per axis: (order key << 32) | first index of the minimum
+    int max_cell[3];               // max lattice index per axis (>= 0: starts at 0 like the reference)
+    int min_cell[3];               // min lattice index per axis (starts at INT_MAX)
+    unsigned int nonfinite;        // inputs that are NaN or +-inf
+    unsigned int mse_max_bits;     // max per-point squared error (float bits)
+    double mse_sum;                // sum of per-point squared errors
+    unsigned int err;              // device error bits
+    float offset[3];               // shift offset (written by quantize_range)
+};
+
+// Key layout of block mode.  Normal cells: key = id << 21 | quad << 18 | sfc18.  Cells with
+// z = -1 (the truncated-octahedron edge case) carry `defect_flag` and the id minus
+// `defect_base` so that they sort after all other cells in the reference's id order.
+struct BlockKeyParams {
+    unsigned long long nx, ny;
+    unsigned long long defect_flag;  // 0 if no z = -1 cells
+    unsigned long long defect_base;  // ((2^64-1)/64/2) * nx * ny  (mod 2^64)
+    int hilbert;
+    unsigned int hstart;  // Hilbert state after levels 20..6 (all zero digits)
+};
+
+// Key layout of direct mode: key = sfc, or defect_flag | (sfc & (defect_flag - 1)) for z = -1
+// cells whose high sfc bits equal `defect_high`.
+struct DirectKeyParams {
+    int bits;      // hilbert_bits = bit length of the max range (>= 1)
+    int hilbert;
+    unsigned long long defect_flag;
+    unsigned long long defect_high;
+};
+
+// Unit (unique cell, or point for -normal) outputs of the segment kernels.
+struct UnitOutputs {
+    uint8_t* rep_sym;               // PFor symbol of repos / sfc delta per unit
+    uint8_t* quad_sym;              // PFor symbol of the quad delta per unit (block mode)
+    unsigned long long* patches;    // PFor patches in order
+    unsigned long long* blk_id;     // block mode: id of each block
+    uint32_t* blk_unit;             // block mode: first unit of each block
+    uint32_t* unit_pos;             // -rle: sorted position of each unit's first point
+    unsigned long long* hist_rep;   // [256]
+    uint32_t* first_rep;            // [256]
+    unsigned long long* hist_quad;  // [256]
+    uint32_t* first_quad;           // [256]
+    unsigned long long* counters;   // [0] units, [1] patches, [2] blocks, [3] sum of patches
+};
+
+struct LookBackState {
+    uint32_t* flag;
+    unsigned long long* agg;
+    unsigned long long* inc;
+};
+
+// Count-stream statistics (-rle).
+constexpr int kCountDense = 4096;
+struct CountStats {
+    unsigned long long* hist;   // [kCountDense]
+    uint32_t* first;            // [kCountDense]
+    uint32_t* over_val;         // counts >= kCountDense: value
+    uint32_t* over_unit;        //   ... and unit index
+    uint32_t* over_n;           // number of such counts
+};
+
+// Huffman code table for uint8 symbols, and for int counts (dense part + sorted sparse part).
+struct ByteCodes {
+    uint32_t bits[256];
+    uint8_t len[256];
+};
+
+struct EncodeTotals {
+    unsigned long long bits[8];  // total bits per stream (see Stream enum in pipeline.cpp)
+};
+
+// --- points ---------------------------------------------------------------------------
+void launch_bbox(const float* xyz, uint64_t n, PointStats* stats, cudaStream_t st);
+void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
+                           cudaStream_t st);
+void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, BlockKeyParams kp,
+                       const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
+                       uint32_t* hist, cudaStream_t st);
+void launch_keys_direct(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, DirectKeyParams kp,
+                        const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
+                        uint32_t* hist, cudaStream_t st);
+void launch_quantize_cells(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, int32_t* cells,
+                           cudaStream_t st);
+void launch_recover_cells(const int32_t* cells, uint64_t n, QuantParams q, const float* offset3_dev, float* xyz,
+                          cudaStream_t st);
+void launch_hilbert(const unsigned long long* in, uint64_t n, const uint8_t* tab, int top, unsigned int state,
+                    unsigned long long* out, cudaStream_t st);
+
+// --- sort -----------------------------------------------------------------------------
+constexpr int kSortTile = 4096;
+void launch_sort_histogram(const unsigned long long* keys, uint64_t n, int passes, uint32_t* hist, cudaStream_t st);
+void launch_sort_offsets(uint32_t* hist, int passes, cudaStream_t st);  // in place: counts -> exclusive offsets
+void launch_sort_pass(const unsigned long long* kin, unsigned long long* kout, const uint32_t* vin, uint32_t* vout,
+                      uint64_t n, int shift, const uint32_t* offsets, unsigned long long* status, uint32_t epoch,
+                      uint32_t* tile_counter, uint32_t* err, cudaStream_t st);
+
+// --- compress segments + encoders -------------------------------------------------------
+constexpr int kUnitTile = 4096;
+void launch_units_block(const unsigned long long* keys, uint64_t n, int rle, BlockKeyParams kp, UnitOutputs out,
+                        LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st);
+void launch_units_direct(const unsigned long long* keys, uint64_t n, int rle, DirectKeyParams kp, UnitOutputs out,
+                         LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st);
+void launch_count_stats(const uint32_t* unit_pos, uint64_t units, uint64_t n, int32_t* counts, CountStats cs,
+                        cudaStream_t st);
+// Block deltas (blk ids and block unit counts) and their maxima.
+void launch_block_deltas(const unsigned long long* blk_id, const uint32_t* blk_unit, uint64_t nblocks, uint64_t units,
+                         unsigned long long* d_blk, unsigned long long* d_cnt, unsigned long long* max2,
+                         cudaStream_t st);
+void launch_bitpack(const unsigned long long* vals, uint64_t n, int width, uint32_t* words, cudaStream_t st);
+
+constexpr int kEncTile = 4096;
+// Encoders write at most cap_bits bits (the output buffer's size) and flag an overflow beyond.
+void launch_gr_encode(const unsigned long long* vals, uint64_t n, int k, uint32_t* words, uint64_t cap_bits,
+                      LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits, uint32_t* err,
+                      cudaStream_t st);
+void launch_huff_encode_u8(const uint8_t* sym, uint64_t n, const ByteCodes* codes, uint32_t* words,
+                           uint64_t cap_bits, LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits,
+                           uint32_t* err, cudaStream_t st);
+// counts: Huffman (eg_k < 0) with a dense table [kCountDense] and sorted sparse values, or
+// exp-Golomb with parameter eg_k >= 0.
+void launch_count_encode(const int32_t* counts, uint64_t n, int eg_k, const uint32_t* dense_bits,
+                         const uint8_t* dense_len, const uint32_t* sparse_val, const uint32_t* sparse_bits,
+                         const uint8_t* sparse_len, uint32_t sparse_n, uint32_t* words, uint64_t cap_bits,
+                         LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits, uint32_t* err,
+                         cudaStream_t st);
+
+// --- decompress -------------------------------------------------------------------------
+void launch_bitunpack(const uint32_t* words, uint64_t base_bits, uint64_t n, int width, unsigned long long* vals,
+                      cudaStream_t st);
+// Inclusive (exclusive = 0) or exclusive prefix sums of u64 values (wrapping), in place allowed.
+constexpr int kScanTile = 4096;
+void launch_scan_u64(const unsigned long long* in, unsigned long long* out, uint64_t n, int exclusive,
+                     LookBackState lb, uint32_t* tile_counter, unsigned long long* total, uint32_t* err,
+                     cudaStream_t st);
+
+// Parallel decoding of one unindexed prefix-code stream (Huffman, Golomb-Rice, exp-Golomb).
+enum CodeKind { kCodeHuffman = 0, kCodeGolombRice = 1, kCodeExpGolomb = 2 };
+struct DecodeTable {
+    // Huffman: primary table of 2^root_bits entries: (len << 24) | symbol for codes of at
+    // most root_bits bits, 0 for a prefix that is no code, (1u << 31) | node for longer
+    // codes; tree nodes hold two children each (leaf = (1u << 31) | symbol, internal = node
+    // index, missing = 0xffffffff).
+    const uint32_t* root;
+    const uint32_t* tree;
+    const unsigned long long* symvals;  // symbol values; table entries hold indices into it
+    int root_bits;
+    int param;   // Golomb-Rice / exp-Golomb k
+    int zigzag;  // exp-Golomb of a signed symbol type
+};
+constexpr int kDecodeMaxL = 64;       // longest entry offset tracked per subsequence
+constexpr int kDecodeSubBits = 512;   // bits per subsequence (thread)
+constexpr int kDecodeBlockSubs = 256; // subsequences per thread block
+size_t decode_smem_bytes();
+// flag: [tiles]; agg: [tiles * kDecodeMaxL]; inc: [tiles * 2]; tiles = ceil(ceil(bits/512)/256)
+// The stream starts `base_bits` into `words`.  L = entry offsets tracked (longest codeword);
+// for Golomb-Rice pass L_run (device: longest run of ones) to derive L on the device.
+void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t,
+                          int L, const uint32_t* L_run, uint64_t nsym, int out_width, void* out, uint32_t* flag,
+                          unsigned long long* agg, unsigned long long* inc, uint32_t* tile_counter, uint32_t* err,
+                          uint32_t* need_fallback, unsigned long long* total_codewords, cudaStream_t st);
+// One-thread decoder used when a codeword longer than the tracked entry range crosses a
+// subsequence boundary.
+void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,
+                              DecodeTable t, uint64_t nsym, int out_width, void* out,
+                              unsigned long long* total_codewords, uint32_t* err, cudaStream_t st);
+void launch_max_ones_run(const uint32_t* words, uint64_t nwords, uint32_t* out, cudaStream_t st);
+void launch_count_total(const int32_t* counts, uint64_t n, unsigned long long* total, cudaStream_t st);
+void launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cudaStream_t st);
+void launch_fill_u8(uint8_t* p, uint64_t n, uint8_t v, cudaStream_t st);
+void launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st);
+
+// LCP recovery (block mode) or SFC prefix sum (direct mode) fused with the PFor decode,
+// -rle expansion, recover and unshift.
+struct RecoverParams {
+    QuantParams q;
+    float off[3];
+    unsigned long long nx, ny;
+    int hilbert;
+    unsigned int hstart_inv;  // inverse-Hilbert state after levels 20..6 of zero digits
+    int rle;
+    int direct;
+    int bits;  // direct mode hilbert_bits
+};
+struct RecoverInputs {
+    const uint8_t* rep_sym;
+    const unsigned long long* rep_patch;
+    uint64_t npatch;
+    const uint8_t* quad_sym;
+    const uint8_t* is_start;       // block mode: 1 where a non-empty block starts
+    const uint32_t* start_block;   // block mode: block index at those units
+    const unsigned long long* blk_ids;
+    uint64_t nblocks;
+    const int32_t* counts;         // -rle
+};
+void launch_block_starts(const unsigned long long* start_excl, uint64_t nblocks, uint64_t units, uint8_t* is_start,
+                         uint32_t* start_block, uint32_t* err, cudaStream_t st);
+// flag: [5 * tiles]; agg, inc: [10 * tiles]; tiles = ceil(units / 4096)
+void launch_recover_units(const RecoverInputs& in, uint64_t units, uint64_t nout, RecoverParams rp,
+                          const uint8_t* hilbert_inv_tab, uint32_t* flag, unsigned long long* agg,
+                          unsigned long long* inc, uint32_t* tile_counter, float* out, uint32_t* err,
+                          cudaStream_t st);
+
+}  // namespace dev
+}  // namespace xnyz
