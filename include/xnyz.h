@@ -143,6 +143,16 @@ xnyz_status xnyz_stage_hilbert(xnyz_ctx* ctx, const uint64_t* dev_in, uint64_t n
  * payload; results replace the inputs. */
 xnyz_status xnyz_stage_sort(xnyz_ctx* ctx, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits);
 
+/* ---- profiling ---------------------------------------------------------------------------- */
+
+/* Enables (1) or disables (0) per-stage CUDA-event timing on the context's stream and clears
+ * what was recorded. */
+xnyz_status xnyz_profile(xnyz_ctx* ctx, int enable);
+/* Synchronises the stream and writes a JSON object {stage: {"ms", "launches", "calls",
+ * "bytes"}} of everything recorded since the last read (bytes = algorithmic traffic); *len
+ * receives the full length.  Clears the record. */
+xnyz_status xnyz_profile_read(xnyz_ctx* ctx, char* json, uint64_t cap, uint64_t* len);
+
 /* ---- host-side helpers (no GPU needed) ----------------------------------------------- */
 
 /* The table-driven Hilbert transform the kernels use, evaluated on the host

@@ -58,6 +58,17 @@ class Context:
         except Exception:
             pass
 
+    # -- profiling --------------------------------------------------------------------
+    def profile(self, enable: bool = True):
+        N.check(N.profile(self.handle, int(enable)))
+
+    def profile_read(self) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        ln = C.c_uint64()
+        N.check(N.profile_read(self.handle, buf, len(buf), C.byref(ln)))
+        return json.loads(buf.value.decode())
+
     # -- whole path -------------------------------------------------------------------
     def compress(self, points, quantizer: int, l2: float, hilbert: bool, rle: bool, direct_threshold: int = 1024,
                  use_zstd: bool = True, want_order: bool = False):

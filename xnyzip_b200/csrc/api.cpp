@@ -119,6 +119,17 @@ struct xnyz_ctx {
     uint8_t* d_container = nullptr;  // device container returned by xnyz_compress_device
     size_t d_container_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // stage profiling (xnyz_profile / xnyz_profile_read)
+    bool prof = false;
+    struct ProfRec {
+        const char* name;
+        cudaEvent_t a, b;
+        uint64_t launches;
+        double bytes;
+    };
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
 };
 
 namespace {
@@ -145,6 +156,38 @@ xnyz_status ensure_host_stage(xnyz_ctx* c, size_t bytes) {
     c->h_stage_cap = want;
     return XNYZ_OK;
 }
+
+cudaEvent_t pool_event(xnyz_ctx* c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+// Brackets one stage's kernel launches with CUDA events on the context's stream when
+// profiling is on.  `launches` counts the kernels, `bytes` their algorithmic traffic.
+struct Prof {
+    xnyz_ctx* c;
+    const char* name;
+    uint64_t launches;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    Prof(xnyz_ctx* cc, const char* nm, uint64_t l, double b) : c(cc), name(nm), launches(l), bytes(b) {
+        if (c->prof && (a = pool_event(c))) cudaEventRecord(a, c->stream);
+    }
+    void end() {
+        if (!c->prof || !a) return;
+        cudaEvent_t e = pool_event(c);
+        if (e) {
+            cudaEventRecord(e, c->stream);
+            c->prof_recs.push_back(xnyz_ctx::ProfRec{name, a, e, launches, bytes});
+        }
+        a = nullptr;
+    }
+    ~Prof() { end(); }
+};
 
 template <typename T>
 T* at(xnyz_ctx* c, size_t off) {
@@ -224,6 +267,7 @@ xnyz_status radix_sort(xnyz_ctx* c, SortBufs& b, uint64_t n, int passes, uint32_
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
         const uint32_t epoch = ++c->sort_epoch;
+        Prof pr(c, "sort_pass", 1, (b.vals[0] ? 24.0 : 16.0) * n);
         launch_sort_pass(b.keys[cur], b.keys[cur ^ 1], b.vals[cur], b.vals[cur ^ 1], n, 8 * p, d_hist + 256 * p,
                          c->sort_status, epoch, SMALL_FIELD(c, tile_counters[p]), SMALL_FIELD(c, err), c->stream);
         cur ^= 1;
@@ -351,8 +395,14 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         CUDA_TRY(cudaMemcpyAsync(&c->d_small->stats, &c->h_small->stats, sizeof(PointStats), cudaMemcpyHostToDevice, st));
         TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
     }
-    launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
-    launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+    {
+        Prof pr(c, "bbox", 1, 12.0 * n);
+        launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
+    }
+    {
+        Prof pr(c, "quantize_range", 1, 12.0 * n);
+        launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+    }
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, stats), sizeof(PointStats)));
     const PointStats S = c->h_small->stats;
@@ -428,12 +478,15 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     TRY(memset_small(c, offsetof(Small, sort_hist), sizeof(uint32_t) * 8 * 256, 0));
     CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_fwd, hm.fwd.data(), 256, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_inv, hm.inv.data(), 256, cudaMemcpyHostToDevice, st));
-    if (direct)
-        launch_keys_direct(d_xyz, n, q, SMALL_FIELD(c, stats), dkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
-                           passes, c->d_small->sort_hist, st);
-    else
-        launch_keys_block(d_xyz, n, q, SMALL_FIELD(c, stats), bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0], passes,
-                          c->d_small->sort_hist, st);
+    {
+        Prof pr(c, "keys", 1, 20.0 * n + (want_order ? 4.0 * n : 0.0));
+        if (direct)
+            launch_keys_direct(d_xyz, n, q, SMALL_FIELD(c, stats), dkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
+                               passes, c->d_small->sort_hist, st);
+        else
+            launch_keys_block(d_xyz, n, q, SMALL_FIELD(c, stats), bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
+                              passes, c->d_small->sort_hist, st);
+    }
     int res = 0;
     TRY(radix_sort(c, sb, n, passes, c->d_small->sort_hist, res));
     const unsigned long long* sorted = sb.keys[res];
@@ -459,12 +512,15 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     uo.hist_quad = c->d_small->hist_quad;
     uo.first_quad = c->d_small->first_quad;
     uo.counters = c->d_small->counters;
-    if (direct)
-        launch_units_direct(sorted, n, rle, dkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
-                            SMALL_FIELD(c, err), st);
-    else
-        launch_units_block(sorted, n, rle, bkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
-                           SMALL_FIELD(c, err), st);
+    {
+        Prof pr(c, "units", 1, 8.0 * n);
+        if (direct)
+            launch_units_direct(sorted, n, rle, dkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
+                                SMALL_FIELD(c, err), st);
+        else
+            launch_units_block(sorted, n, rle, bkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
+                               SMALL_FIELD(c, err), st);
+    }
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, counters), sizeof(unsigned long long) * 8));
     const uint64_t U = c->h_small->counters[0], P = c->h_small->counters[1], NB = c->h_small->counters[2];
@@ -478,10 +534,12 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         TRY(memset_small(c, offsetof(Small, over_n), sizeof(uint32_t), 0));
         CountStats cs{c->d_small->cnt_hist, c->d_small->cnt_first, at<uint32_t>(c, o_over_v), at<uint32_t>(c, o_over_u),
                       SMALL_FIELD(c, over_n)};
+        Prof pr(c, "count_stats", 1, 8.0 * U);
         launch_count_stats(uo.unit_pos, U, n, at<int32_t>(c, o_counts), cs, st);
     }
     if (!direct) {
         TRY(memset_small(c, offsetof(Small, max2), sizeof(unsigned long long) * 2, 0));
+        Prof pr(c, "block_deltas", 1, 28.0 * NB);
         launch_block_deltas(uo.blk_id, uo.blk_unit, NB, U, at<unsigned long long>(c, o_dblk),
                             at<unsigned long long>(c, o_dcnt), c->d_small->max2, st);
     }
@@ -599,9 +657,12 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         return LookBackState{lbs.flag + ch * lb_enc.tiles, lbs.agg + ch * lb_enc.tiles, lbs.inc + ch * lb_enc.tiles};
     };
     if (!direct) {
+        Prof pr(c, "bitpack", 2, 16.0 * NB + (w_blk + w_cnt) * NB / 8.0);
         launch_bitpack(at<unsigned long long>(c, o_dblk), NB, w_blk, at<uint32_t>(c, o_w_blk), st);
         launch_bitpack(at<unsigned long long>(c, o_dcnt), NB, w_cnt, at<uint32_t>(c, o_w_cnt), st);
     }
+    Prof pr_enc(c, "entropy_encode", (P ? 1 : 0) + (code_rep.exp_golomb ? 0 : 1) + (direct ? 0 : 1) + (rle ? 1 : 0),
+                8.0 * P + bits_gr / 8.0 + 2.0 * U + (bits_rep + bits_quad + bits_cnt) / 8.0 + (rle ? 4.0 * U : 0.0));
     launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
                      SMALL_FIELD(c, tile_counters[0]),
                      SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), st);
@@ -632,6 +693,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
                             SMALL_FIELD(c, tile_counters[3]), SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), st);
     }
     CUDA_TRY(cudaGetLastError());
+    pr_enc.end();
     TRY(fetch_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8));
     TRY(check_device_errors(c));
     const uint64_t gr_bits = c->h_small->totals[0];
@@ -968,6 +1030,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         uint64_t b0, b1;
         const uint32_t* w0 = words_of(h.streams[0], b0);
         const uint32_t* w1 = words_of(h.streams[1], b1);
+        Prof pr(c, "block_streams", 6, 16.0 * NB + (w_blk + w_cnt) * NB / 8.0 + 48.0 * NB + 9.0 * NB);
         launch_bitunpack(w0, b0, NB, w_blk, at<unsigned long long>(c, o_blkd), st);
         launch_bitunpack(w1, b1, NB, w_cnt, at<unsigned long long>(c, o_cntd), st);
         TRY(lb_clear(c, lb_scan, 3));
@@ -1051,6 +1114,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                 launch_fill_u32(static_cast<uint32_t*>(j.out), j.nsym, static_cast<uint32_t>(j.fill_value), st);
             continue;
         }
+        Prof pr(c, j.kind == kCodeGolombRice ? "decode_golomb_rice" : (j.kind == kCodeHuffman ? "decode_huffman" : "decode_exp_golomb"),
+                j.kind == kCodeGolombRice ? 2 : 1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width);
         const uint32_t* Lrun = nullptr;
         if (j.kind == kCodeGolombRice) {
             const uint64_t w_first = j.base_bits / 32, nw = cdiv(j.base_bits + j.total_bits, 32) - w_first;
@@ -1078,7 +1143,10 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         }
     }
     (void)refetch;
-    if (rle && U) launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
+    if (rle && U) {
+        Prof pr(c, "count_total", 1, 4.0 * U);
+        launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
+    }
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, totals), offsetof(Small, tile_counters) - offsetof(Small, totals)));
     TRY(check_device_errors(c));
@@ -1127,10 +1195,13 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     ri.counts = at<int32_t>(c, o_counts);
     CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_rflag), 0, 4 * rtiles * 5, st));
     float* out = at<float>(c, o_out);
+    Prof pr_rec(c, "recover_units", 1,
+                (h.direct ? 1.0 : 7.0) * U + 8.0 * P + (rle ? 4.0 * U : 0.0) + 12.0 * static_cast<double>(nout));
     launch_recover_units(ri, U, nout, rp, c->d_small->hil_inv, at<uint32_t>(c, o_rflag),
                          at<unsigned long long>(c, o_ragg), at<unsigned long long>(c, o_rinc),
                          SMALL_FIELD(c, tile_counters[40]), out, SMALL_FIELD(c, err), st);
     CUDA_TRY(cudaGetLastError());
+    pr_rec.end();
     TRY(check_device_errors(c));
     *d_out = out;
     *n_out = nout;
@@ -1209,6 +1280,7 @@ xnyz_status xnyz_destroy(xnyz_ctx* c) {
     if (c->h_small) cudaFreeHost(c->h_small);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->d_container) cudaFree(c->d_container);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -1497,6 +1569,55 @@ xnyz_status xnyz_stage_sort(xnyz_ctx* c, uint64_t* dev_keys, uint32_t* dev_paylo
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return check_device_errors(c);
+}
+
+xnyz_status xnyz_profile(xnyz_ctx* c, int enable) {
+    if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
+    c->prof = enable != 0;
+    c->prof_recs.clear();
+    c->ev_used = 0;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_profile_read(xnyz_ctx* c, char* json, uint64_t cap, uint64_t* len) {
+    if (!c || !len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    struct Agg {
+        double ms = 0, bytes = 0;
+        uint64_t launches = 0, calls = 0;
+    };
+    std::map<std::string, Agg> agg;
+    for (const auto& r : c->prof_recs) {
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, r.a, r.b));
+        Agg& a = agg[r.name];
+        a.ms += ms;
+        a.bytes += r.bytes;
+        a.launches += r.launches;
+        a.calls += 1;
+    }
+    std::string out = "{";
+    bool first = true;
+    for (const auto& kv : agg) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "%s\"%s\": {\"ms\": %.6f, \"launches\": %llu, \"calls\": %llu, \"bytes\": %.1f}",
+                      first ? "" : ", ", kv.first.c_str(), kv.second.ms,
+                      static_cast<unsigned long long>(kv.second.launches),
+                      static_cast<unsigned long long>(kv.second.calls), kv.second.bytes);
+        out += buf;
+        first = false;
+    }
+    out += "}";
+    *len = out.size();
+    if (json && cap) {
+        const size_t k = std::min<size_t>(cap - 1, out.size());
+        std::memcpy(json, out.data(), k);
+        json[k] = 0;
+    }
+    c->prof_recs.clear();
+    c->ev_used = 0;
+    return XNYZ_OK;
 }
 
 xnyz_status xnyz_host_hilbert(const uint64_t* in, uint64_t n, unsigned iteration, int inverse, uint64_t* out) {

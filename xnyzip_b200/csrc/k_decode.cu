@@ -714,7 +714,8 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
 
     // ---- final: coordinates, recover, unshift, expand ----
     const QuantParams q = a.rp.q;
-    u64 opos = base_count + ec;
+    // -rle: output position from the count prefix; -normal: one point per unit.
+    u64 opos = rle ? base_count + ec : base + e0;
     u64 sfc = base_sfc + ed;
     Seg qrun = op(base_quad, eq), brun = op(base_blk, eb), rrun = op(base_rep, er);
     for (int i = 0; i < kItems; ++i) {
