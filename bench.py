@@ -120,7 +120,10 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated stream shared with the library: the timing events below are recorded on
+    # the stream the kernels are launched on.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx = X.Context(local, stream=stream.cuda_stream)
 
     n = args.points
@@ -168,8 +171,10 @@ def run_gpu(args):
         clens = device_step()
     ev1.record(stream)
     torch.cuda.synchronize(dev)
-    prof = ctx.profile_read()
+    prof_all = ctx.profile_read()
     ctx.profile(False)
+    prof = {k: v for k, v in prof_all.items() if not k.startswith("host:")}
+    host_phases = {k[5:]: round(v["ms"] / args.steps, 3) for k, v in prof_all.items() if k.startswith("host:")}
     clk = clocks.stop()
     dev_ms = ev0.elapsed_time(ev1)
     dev_ms = max_over_ranks(dev_ms)
@@ -191,11 +196,14 @@ def run_gpu(args):
         e2e_step()
     barrier()
     torch.cuda.synchronize(dev)
+    ctx.profile(True)
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize(dev)
     e2e_s = max_over_ranks(time.perf_counter() - w0)
+    e2e_prof = {k[5:]: round(v["ms"] / e2e_steps, 2) for k, v in ctx.profile_read().items() if k.startswith("host:")}
+    ctx.profile(False)
 
     # ---- CPU baseline: the reference on a bounded sample (rank 0, N = 1) ----
     cpu = None
@@ -245,7 +253,7 @@ def run_gpu(args):
             "bits_per_point": bpp,
             "e2e": {"value": round(e2e, 4), "unit": "GB/s", "h2d_bytes_per_step": int(12 * n * len(variants)),
                     "d2h_bytes_per_step": int(12 * n * len(variants)), "steps": e2e_steps,
-                    "s_per_step": round(e2e_s / e2e_steps, 4)},
+                    "s_per_step": round(e2e_s / e2e_steps, 4), "host_phases_ms_per_step": e2e_prof},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": None,
@@ -255,6 +263,7 @@ def run_gpu(args):
             "stages": {k: {"ms_per_step": round(v["ms"] / args.steps, 4), "launches": v["launches"] // args.steps,
                            "GB_s": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None}
                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
+            "host_phases_ms_per_step": host_phases,
             "gpu_launches": int(launches),
             "clocks": clk,
         }

@@ -130,6 +130,7 @@ struct xnyz_ctx {
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
+    std::map<std::string, std::pair<double, uint64_t>> host_ms;  // host phase wall time, calls
 };
 
 namespace {
@@ -187,6 +188,24 @@ struct Prof {
         a = nullptr;
     }
     ~Prof() { end(); }
+};
+
+// Wall time of a host phase (including the device work it waits for) when profiling.
+struct HostPhase {
+    xnyz_ctx* c;
+    const char* name;
+    std::chrono::steady_clock::time_point t0;
+    bool open = true;
+    HostPhase(xnyz_ctx* cc, const char* nm) : c(cc), name(nm), t0(std::chrono::steady_clock::now()) {}
+    void end() {
+        if (!open) return;
+        open = false;
+        if (!c->prof) return;
+        auto& e = c->host_ms[name];
+        e.first += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        e.second += 1;
+    }
+    ~HostPhase() { end(); }
 };
 
 template <typename T>
@@ -383,6 +402,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     cudaStream_t st = c->stream;
 
     // ---- 1. bounding box + quantization sweep ----
+    HostPhase hp1(c, "c1_stats");
     {
         PointStats init{};
         for (int a = 0; a < 3; ++a) {
@@ -406,6 +426,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, stats), sizeof(PointStats)));
     const PointStats S = c->h_small->stats;
+    hp1.end();
+    HostPhase hp2(c, "c2_keys_sort_units");
     if (S.nonfinite) return fail(XNYZ_ERR_UNSUPPORTED, "input contains NaN or infinite coordinates");
     if (S.min_cell[0] < 0 || S.min_cell[1] < 0 || S.min_cell[2] < -1)
         return fail(XNYZ_ERR_UNSUPPORTED, "lattice index outside the int range (coordinates too large for the bound)");
@@ -526,6 +548,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     const uint64_t U = c->h_small->counters[0], P = c->h_small->counters[1], NB = c->h_small->counters[2];
     const uint64_t psum = c->h_small->counters[3];
     TRY(check_device_errors(c));
+    hp2.end();
+    HostPhase hp3(c, "c3_stats");
 
     // ---- 6. count and block statistics ----
     if (rle) {
@@ -547,6 +571,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     TRY(fetch_small(c, offsetof(Small, hist_rep),
                     offsetof(Small, tile_counters) - offsetof(Small, hist_rep)));  // hists, counts, maxima
     const Small& H = *c->h_small;
+    hp3.end();
+    HostPhase hp4(c, "c4_codebooks");
 
     // ---- 7. codebooks (host replay of the reference's container order) ----
     std::vector<SymbolStat> st_rep, st_quad, st_cnt;
@@ -622,6 +648,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         w_cnt = H.max2[1] == 0 ? 1 : bitlen(H.max2[1]);
     }
 
+    hp4.end();
+    HostPhase hp5(c, "c5_encode");
     // ---- 8. encoders ----
     // Output sizes: Huffman and bit-pack streams are known exactly; the Golomb-Rice stream is
     // bounded by P*(k+1) + sum(v >> k) <= P*(k+1) + (sum >> k) + P.
@@ -702,6 +730,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     if (!direct && c->h_small->totals[2] != bits_quad) return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (quads)");
     if (rle && c->h_small->totals[3] != bits_cnt) return fail(XNYZ_ERR_CUDA, "count encoder size mismatch");
 
+    hp5.end();
+    HostPhase hp6(c, "c6_container");
     // ---- 9. container (Appendix: block_compressor.hpp:56-215, block_compressor_rle.hpp:125-314) ----
     Container& K = R.cont;
     K.pod<uint64_t>(U);
@@ -926,6 +956,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         return reinterpret_cast<const uint32_t*>(d_cont + (s.data_off & ~static_cast<uint64_t>(3)));
     };
 
+    HostPhase hd1(c, "d1_metas_tables");
     // ---- stream metas ----
     const int i_gr = h.direct ? 0 : 2, i_sym = h.direct ? 1 : 3;
     const StreamRef& s_gr = h.streams[i_gr];
@@ -1025,6 +1056,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(upload(ht_quad, to_quad));
     TRY(upload(ht_cnt, to_cnt));
 
+    hd1.end();
+    HostPhase hd2(c, "d2_launch");
     // ---- block streams: bit-unpack + prefix sums ----
     if (!h.direct && NB) {
         uint64_t b0, b1;
@@ -1130,6 +1163,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                              st);
     }
     CUDA_TRY(cudaGetLastError());
+    hd2.end();
+    HostPhase hd3(c, "d3_decode_sync");
     // count total (for -rle) after the count stream is decoded
     TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
     TRY(fetch_small(c, offsetof(Small, fallback), sizeof(uint32_t) * 8));
@@ -1157,6 +1192,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         return fail(XNYZ_ERR_BAD_STREAM, "block counts do not add up to the point count");
     if (!h.direct && NB == 0 && U) return fail(XNYZ_ERR_BAD_STREAM, "no blocks");
     const uint64_t nout = rle ? c->h_small->totals[0] : U;
+    hd3.end();
+    HostPhase hd4(c, "d4_recover");
 
     // ---- output buffer (after the arena's planned part) ----
     Plan po;
@@ -1358,6 +1395,7 @@ xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_
         for (uint64_t i = 0; i < n; ++i) sort_order[i] = order[i];
     uint8_t* buf = nullptr;
     uint64_t blen = 0;
+    HostPhase hz(c, "c8_zstd");
     if (use_zstd) {
         std::string e;
         const size_t cap = zstd_bound(clen);
@@ -1396,6 +1434,7 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
     CompressOut R;
     TRY(ensure_arena(c, make_cplan(n, false, 0).total + encoder_reserve(n)));
     TRY(compress_run(c, xyz, n, *params, false, 0, R));
+    HostPhase hpa(c, "c7_assemble_device");
     const size_t clen = R.cont.skel.size();
     if (c->d_container_cap < clen + 64) {
         CUDA_TRY(cudaStreamSynchronize(st));
@@ -1435,6 +1474,7 @@ xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int
     const uint8_t* raw = in;
     uint64_t len = in_len;
     std::string e;
+    HostPhase hu(c, "d0_unzstd_header");
     if (is_zstd) {
         uint64_t fs = 0;
         if (!zstd_content_size(in, in_len, fs, e)) return fail(XNYZ_ERR_ZSTD, e);
@@ -1446,6 +1486,7 @@ xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int
     Header h;
     TRY(parse_header([&](uint64_t off, uint64_t bytes, void* dst) { std::memcpy(dst, raw + off, bytes); return true; },
                      len, rle != 0, h));
+    hu.end();
     const size_t reserved = align_up(len + 64);
     TRY(ensure_arena(c, reserved));
     CUDA_TRY(cudaMemcpyAsync(c->arena.base, raw, len, cudaMemcpyHostToDevice, st));
@@ -1454,6 +1495,7 @@ xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int
     uint64_t nout = 0;
     TRY(decompress_run(c, reinterpret_cast<const uint8_t*>(c->arena.base), len, h, quantizer, l2_bound, rle != 0,
                        reserved, &d_out, &nout));
+    HostPhase hdh(c, "d5_d2h");
     float* host = static_cast<float*>(std::malloc(12 * nout + 4));
     if (!host) return fail(XNYZ_ERR_OOM, "host allocation");
     if (nout) CUDA_TRY(cudaMemcpyAsync(host, d_out, 12 * nout, cudaMemcpyDeviceToHost, st));
@@ -1482,6 +1524,7 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
         d_cont = reinterpret_cast<const uint8_t*>(c->arena.base);
     }
     Header h;
+    HostPhase hph(c, "d0_header_device");
     xnyz_status s = parse_header(
         [&](uint64_t off, uint64_t bytes, void* dst) {
             return cudaMemcpyAsync(dst, d_cont + off, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
@@ -1489,6 +1532,7 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
         },
         len, rle != 0, h);
     if (s != XNYZ_OK) return s;
+    hph.end();
     float* d_out = nullptr;
     uint64_t nout = 0;
     TRY(decompress_run(c, d_cont, len, h, quantizer, l2_bound, rle != 0, reserved, &d_out, &nout));
@@ -1575,6 +1619,7 @@ xnyz_status xnyz_profile(xnyz_ctx* c, int enable) {
     if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
     c->prof = enable != 0;
     c->prof_recs.clear();
+    c->host_ms.clear();
     c->ev_used = 0;
     return XNYZ_OK;
 }
@@ -1608,6 +1653,14 @@ xnyz_status xnyz_profile_read(xnyz_ctx* c, char* json, uint64_t cap, uint64_t* l
         out += buf;
         first = false;
     }
+    for (const auto& kv : c->host_ms) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s\"host:%s\": {\"ms\": %.6f, \"launches\": 0, \"calls\": %llu, \"bytes\": 0}",
+                      first ? "" : ", ", kv.first.c_str(), kv.second.first,
+                      static_cast<unsigned long long>(kv.second.second));
+        out += buf;
+        first = false;
+    }
     out += "}";
     *len = out.size();
     if (json && cap) {
@@ -1616,6 +1669,7 @@ xnyz_status xnyz_profile_read(xnyz_ctx* c, char* json, uint64_t cap, uint64_t* l
         json[k] = 0;
     }
     c->prof_recs.clear();
+    c->host_ms.clear();
     c->ev_used = 0;
     return XNYZ_OK;
 }
