@@ -143,6 +143,20 @@ xnyz_status xnyz_stage_hilbert(xnyz_ctx* ctx, const uint64_t* dev_in, uint64_t n
  * payload; results replace the inputs. */
 xnyz_status xnyz_stage_sort(xnyz_ctx* ctx, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits);
 
+/* ---- allocation-free entry point ---------------------------------------------------------- */
+
+/* No counterpart in the reference.  The stable LSD radix sort of xnyz_stage_sort for callers
+ * that cannot allocate device memory while they run (a real-time loop that must not block on
+ * the CUDA allocator, a plugin whose host application owns all device memory): no context,
+ * no cudaMalloc / cudaFree; all scratch lives in one fixed device array of about 12.6 MB
+ * that every GPU loading the library holds until exit.  Sorts n <= 2^20 uint64 keys (and an
+ * optional uint32 payload) in place over bits [0, key_bits) on `stream` (a cudaStream_t, NULL
+ * = default stream) on the current device, and waits for the result.  n > 2^20 returns
+ * XNYZ_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address; make
+ * it before any stream capture.  Calls share the array: calls that overlap on the GPU race,
+ * so serialise them. */
+xnyz_status xnyz_sort_noalloc(uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits, void* stream);
+
 /* ---- profiling ---------------------------------------------------------------------------- */
 
 /* Enables (1) or disables (0) per-stage CUDA-event timing on the context's stream and clears

@@ -79,6 +79,7 @@ stage_quantize = _proto("xnyz_stage_quantize", [_p, _p, C.c_uint64, C.c_int, C.c
 stage_recover = _proto("xnyz_stage_recover", [_p, _p, C.c_uint64, C.c_int, C.c_float, _p, _p])
 stage_hilbert = _proto("xnyz_stage_hilbert", [_p, _p, C.c_uint64, C.c_uint, C.c_int, _p])
 stage_sort = _proto("xnyz_stage_sort", [_p, _p, _p, C.c_uint64, C.c_int])
+sort_noalloc = _proto("xnyz_sort_noalloc", [_p, _p, C.c_uint64, C.c_int, _p])
 profile = _proto("xnyz_profile", [_p, C.c_int])
 profile_read = _proto("xnyz_profile_read", [_p, C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)])
 host_hilbert = _proto("xnyz_host_hilbert", [_p, C.c_uint64, C.c_uint, C.c_int, _p])
@@ -90,7 +91,7 @@ EXPORTED = [
     "xnyz_create", "xnyz_destroy", "xnyz_last_error", "xnyz_version", "xnyz_set_zstd_library", "xnyz_host_alloc",
     "xnyz_host_free", "xnyz_trim", "xnyz_compress", "xnyz_compress_device", "xnyz_decompress",
     "xnyz_decompress_device", "xnyz_free", "xnyz_stage_quantize", "xnyz_stage_recover", "xnyz_stage_hilbert",
-    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read",
+    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_sort_noalloc",
 ]
 
 
