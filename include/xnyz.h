@@ -121,6 +121,12 @@ xnyz_status xnyz_compress_device(xnyz_ctx* ctx, const float* xyz, uint64_t n, co
 xnyz_status xnyz_decompress(xnyz_ctx* ctx, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
                             float l2_bound, int rle, float** xyz, uint64_t* n);
 
+/* As xnyz_decompress, into a caller-provided host array of `capacity` points (3 floats each;
+ * pinned memory from xnyz_host_alloc gives the fastest copy).  *n receives the point count;
+ * if it exceeds `capacity` nothing is copied and XNYZ_ERR_INVALID_ARG is returned. */
+xnyz_status xnyz_decompress_into(xnyz_ctx* ctx, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                                 float l2_bound, int rle, float* xyz, uint64_t capacity, uint64_t* n);
+
 /* Decompress a device-resident raw container into a device array owned by the context
  * (valid until the next call).  Host code reads the few header fields it needs. */
 xnyz_status xnyz_decompress_device(xnyz_ctx* ctx, const uint8_t* dev_container, uint64_t len, int quantizer,

@@ -94,8 +94,21 @@ class Context:
         self.last_info = info
         return (data, order[:n]) if want_order else data
 
-    def decompress(self, data: bytes, quantizer: int, l2: float, rle: bool, is_zstd: bool = True) -> np.ndarray:
+    def decompress(self, data: bytes, quantizer: int, l2: float, rle: bool, is_zstd: bool = True,
+                   out: np.ndarray | None = None) -> np.ndarray:
+        """Decoded points as an (n, 3) float32 array.  With `out` (e.g. a view of pinned
+        memory) the points are copied straight into it and a view of its first n rows is
+        returned."""
         buf = np.frombuffer(data, dtype=np.uint8)
+        if out is not None:
+            o = out.reshape(-1, 3)
+            if o.dtype != np.float32 or not o.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float32 array")
+            n = C.c_uint64()
+            N.check(N.decompress_into(self.handle, buf.ctypes.data_as(C.c_void_p), len(data), int(is_zstd),
+                                      int(quantizer), float(l2), int(bool(rle)), o.ctypes.data_as(C.c_void_p),
+                                      o.shape[0], C.byref(n)))
+            return o[: n.value]
         out = C.POINTER(C.c_float)()
         n = C.c_uint64()
         N.check(N.decompress(self.handle, buf.ctypes.data_as(C.c_void_p), len(data), int(is_zstd), int(quantizer),

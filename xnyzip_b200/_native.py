@@ -73,6 +73,8 @@ compress_device = _proto("xnyz_compress_device", [_p, _p, C.c_uint64, C.POINTER(
                                                   C.POINTER(C.c_uint64), C.POINTER(CompressInfo)])
 decompress = _proto("xnyz_decompress", [_p, _p, C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_int,
                                         C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_uint64)])
+decompress_into = _proto("xnyz_decompress_into", [_p, _p, C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_int, _p,
+                                                  C.c_uint64, C.POINTER(C.c_uint64)])
 decompress_device = _proto("xnyz_decompress_device", [_p, _p, C.c_uint64, C.c_int, C.c_float, C.c_int,
                                                       C.POINTER(_p), C.POINTER(C.c_uint64)])
 stage_quantize = _proto("xnyz_stage_quantize", [_p, _p, C.c_uint64, C.c_int, C.c_float, _p, _p])
@@ -91,7 +93,7 @@ EXPORTED = [
     "xnyz_create", "xnyz_destroy", "xnyz_last_error", "xnyz_version", "xnyz_set_zstd_library", "xnyz_host_alloc",
     "xnyz_host_free", "xnyz_trim", "xnyz_compress", "xnyz_compress_device", "xnyz_decompress",
     "xnyz_decompress_device", "xnyz_free", "xnyz_stage_quantize", "xnyz_stage_recover", "xnyz_stage_hilbert",
-    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_sort_noalloc",
+    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_sort_noalloc", "xnyz_decompress_into",
 ]
 
 

@@ -297,27 +297,66 @@ xnyz_status radix_sort(xnyz_ctx* c, SortBufs& b, uint64_t n, int passes, uint32_
 }
 
 // ---------------------------------------------------------------- container --------------
-struct Hole {
-    const void* dsrc;  // device source
-    size_t off;        // offset in the container
-    size_t bytes;
-};
 
+// The container as an ordered list of pieces: header bytes kept on the host (a few KB) and
+// stream payloads left in device memory until the container is assembled where it is needed.
 struct Container {
-    std::vector<uint8_t> skel;  // host bytes (holes zero)
-    std::vector<Hole> holes;
+    struct Piece {
+        size_t off;        // offset in the container
+        size_t len;
+        size_t blob_off;   // host piece: offset in `blob`
+        const void* dsrc;  // device piece: source (nullptr for host pieces)
+    };
+    std::vector<uint8_t> blob;  // all host bytes, in container order
+    std::vector<Piece> pieces;
+    size_t size = 0;
+    void host_bytes(const void* p, size_t n) {
+        if (!n) return;
+        if (!pieces.empty() && !pieces.back().dsrc) {
+            pieces.back().len += n;
+        } else {
+            pieces.push_back(Piece{size, n, blob.size(), nullptr});
+        }
+        const uint8_t* b = static_cast<const uint8_t*>(p);
+        blob.insert(blob.end(), b, b + n);
+        size += n;
+    }
     template <typename V>
     void pod(V v) {
-        const uint8_t* p = reinterpret_cast<const uint8_t*>(&v);
-        skel.insert(skel.end(), p, p + sizeof(V));
+        host_bytes(&v, sizeof(V));
     }
     // [u64 data_len][u64 meta_len][meta][data]  (block_compressor.hpp:152-155)
     void stream(const std::vector<uint8_t>& meta, const void* ddata, size_t data_bytes) {
         pod<uint64_t>(data_bytes);
         pod<uint64_t>(meta.size());
-        skel.insert(skel.end(), meta.begin(), meta.end());
-        if (data_bytes) holes.push_back(Hole{ddata, skel.size(), data_bytes});
-        skel.resize(skel.size() + data_bytes, 0);
+        host_bytes(meta.data(), meta.size());
+        if (data_bytes) {
+            pieces.push_back(Piece{size, data_bytes, 0, ddata});
+            size += data_bytes;
+        }
+    }
+    // Assemble into host memory (device pieces copied asynchronously on `st`).
+    cudaError_t to_host(uint8_t* dst, cudaStream_t st) const {
+        for (const Piece& pc : pieces) {
+            if (pc.dsrc) {
+                const cudaError_t e = cudaMemcpyAsync(dst + pc.off, pc.dsrc, pc.len, cudaMemcpyDeviceToHost, st);
+                if (e != cudaSuccess) return e;
+            } else {
+                std::memcpy(dst + pc.off, blob.data() + pc.blob_off, pc.len);
+            }
+        }
+        return cudaSuccess;
+    }
+    // Assemble into device memory; host pieces are staged through `stage` (pinned, >= blob).
+    cudaError_t to_device(uint8_t* dst, uint8_t* stage, cudaStream_t st) const {
+        std::memcpy(stage, blob.data(), blob.size());
+        for (const Piece& pc : pieces) {
+            const cudaError_t e =
+                pc.dsrc ? cudaMemcpyAsync(dst + pc.off, pc.dsrc, pc.len, cudaMemcpyDeviceToDevice, st)
+                        : cudaMemcpyAsync(dst + pc.off, stage + pc.blob_off, pc.len, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     }
 };
 
@@ -765,7 +804,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     I.num_units = U;
     I.num_blocks = direct ? 0 : NB;
     I.num_patches = P;
-    I.container_bytes = K.skel.size();
+    I.container_bytes = K.size;
     I.range[0] = rx;
     I.range[1] = ry;
     I.range[2] = rz;
@@ -1148,13 +1187,9 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
             continue;
         }
         Prof pr(c, j.kind == kCodeGolombRice ? "decode_golomb_rice" : (j.kind == kCodeHuffman ? "decode_huffman" : "decode_exp_golomb"),
-                j.kind == kCodeGolombRice ? 2 : 1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width);
+                1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width);
+        // Golomb-Rice tracks k + 2 entry offsets per subsequence (derived in the kernel).
         const uint32_t* Lrun = nullptr;
-        if (j.kind == kCodeGolombRice) {
-            const uint64_t w_first = j.base_bits / 32, nw = cdiv(j.base_bits + j.total_bits, 32) - w_first;
-            launch_max_ones_run(j.words, nw, SMALL_FIELD(c, maxrun[j.slot]), st);
-            Lrun = SMALL_FIELD(c, maxrun[j.slot]);
-        }
         CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_dflag[j.slot]), 0, 4 * dtiles, st));
         launch_decode_stream(j.kind, j.words, j.base_bits, j.total_bits, j.table, j.L, Lrun, j.nsym, j.width, j.out,
                              at<uint32_t>(c, o_dflag[j.slot]), at<unsigned long long>(c, o_dagg[j.slot]),
@@ -1379,11 +1414,9 @@ xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_
     const bool want_order = sort_order != nullptr && !params->rle;
     TRY(compress_run(c, d_xyz, n, *params, want_order, reserved, R));
     // container: skeleton on the host, stream bytes copied from the device into place
-    const size_t clen = R.cont.skel.size();
+    const size_t clen = R.cont.size;
     TRY(ensure_host_stage(c, clen));
-    std::memcpy(c->h_stage, R.cont.skel.data(), clen);
-    for (const Hole& hl : R.cont.holes)
-        CUDA_TRY(cudaMemcpyAsync(c->h_stage + hl.off, hl.dsrc, hl.bytes, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(R.cont.to_host(c->h_stage, st));
     std::vector<uint32_t> order;
     if (want_order) {
         order.resize(n);
@@ -1435,7 +1468,7 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
     TRY(ensure_arena(c, make_cplan(n, false, 0).total + encoder_reserve(n)));
     TRY(compress_run(c, xyz, n, *params, false, 0, R));
     HostPhase hpa(c, "c7_assemble_device");
-    const size_t clen = R.cont.skel.size();
+    const size_t clen = R.cont.size;
     if (c->d_container_cap < clen + 64) {
         CUDA_TRY(cudaStreamSynchronize(st));
         if (c->d_container) cudaFree(c->d_container);
@@ -1444,12 +1477,9 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
         CUDA_TRY(cudaMalloc(&c->d_container, want));
         c->d_container_cap = want;
     }
-    TRY(ensure_host_stage(c, clen));
-    std::memcpy(c->h_stage, R.cont.skel.data(), clen);
-    CUDA_TRY(cudaMemcpyAsync(c->d_container, c->h_stage, clen, cudaMemcpyHostToDevice, st));
+    TRY(ensure_host_stage(c, R.cont.blob.size()));
+    CUDA_TRY(R.cont.to_device(c->d_container, c->h_stage, st));
     CUDA_TRY(cudaMemsetAsync(c->d_container + clen, 0, 64, st));
-    for (const Hole& hl : R.cont.holes)
-        CUDA_TRY(cudaMemcpyAsync(c->d_container + hl.off, hl.dsrc, hl.bytes, cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(cudaEventRecord(c->ev1, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     *dev_container = c->d_container;
@@ -1464,9 +1494,12 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
     return XNYZ_OK;
 }
 
-xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
-                            float l2_bound, int rle, float** xyz, uint64_t* n) {
-    if (!c || !in || !xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+namespace {
+// Host-buffer decompress: zstd + header on the host, decode on the device; the points stay
+// in the context's arena (*d_out, *nout) for the caller to copy out.
+xnyz_status decompress_host_input(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                                  float l2_bound, int rle, float** d_out, uint64_t* nout) {
+    if (!c || !in) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
         return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
     CUDA_TRY(cudaSetDevice(c->device));
@@ -1491,17 +1524,47 @@ xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int
     TRY(ensure_arena(c, reserved));
     CUDA_TRY(cudaMemcpyAsync(c->arena.base, raw, len, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemsetAsync(c->arena.base + len, 0, 64, st));
+    return decompress_run(c, reinterpret_cast<const uint8_t*>(c->arena.base), len, h, quantizer, l2_bound, rle != 0,
+                          reserved, d_out, nout);
+}
+}  // namespace
+
+xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                            float l2_bound, int rle, float** xyz, uint64_t* n) {
+    if (!xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     float* d_out = nullptr;
     uint64_t nout = 0;
-    TRY(decompress_run(c, reinterpret_cast<const uint8_t*>(c->arena.base), len, h, quantizer, l2_bound, rle != 0,
-                       reserved, &d_out, &nout));
+    TRY(decompress_host_input(c, in, in_len, is_zstd, quantizer, l2_bound, rle, &d_out, &nout));
+    cudaStream_t st = c->stream;
     HostPhase hdh(c, "d5_d2h");
     float* host = static_cast<float*>(std::malloc(12 * nout + 4));
     if (!host) return fail(XNYZ_ERR_OOM, "host allocation");
-    if (nout) CUDA_TRY(cudaMemcpyAsync(host, d_out, 12 * nout, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    // Through the pinned staging buffer in chunks (a pageable destination is slow to DMA to).
+    const size_t total = 12 * nout, chunk = 64u << 20;
+    TRY(ensure_host_stage(c, std::min(total, 2 * chunk) + 64));
+    for (size_t off = 0, k = 0; off < total; off += chunk, ++k) {
+        const size_t len = std::min(chunk, total - off);
+        uint8_t* buf = c->h_stage + (k & 1) * chunk;
+        CUDA_TRY(cudaMemcpyAsync(buf, reinterpret_cast<const uint8_t*>(d_out) + off, len, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        std::memcpy(reinterpret_cast<uint8_t*>(host) + off, buf, len);
+    }
     *xyz = host;
     *n = nout;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_decompress_into(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
+                                 float l2_bound, int rle, float* xyz, uint64_t capacity, uint64_t* n) {
+    if (!xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    float* d_out = nullptr;
+    uint64_t nout = 0;
+    TRY(decompress_host_input(c, in, in_len, is_zstd, quantizer, l2_bound, rle, &d_out, &nout));
+    *n = nout;
+    if (nout > capacity) return fail(XNYZ_ERR_INVALID_ARG, "output buffer too small (*n holds the point count)");
+    HostPhase hdh(c, "d5_d2h");
+    if (nout) CUDA_TRY(cudaMemcpyAsync(xyz, d_out, 12 * nout, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     return XNYZ_OK;
 }
 

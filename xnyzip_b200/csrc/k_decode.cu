@@ -189,15 +189,17 @@ __device__ __forceinline__ u64 codeword(const Stream& s, u64 p, u64& val) {
 // ------------------------------------------------------------- stream decoder -----------
 constexpr int kMaxL = 64;
 constexpr u32 kOOD = 0xffu;
-constexpr int kSubBits = 512;
-constexpr int kBmWords = kSubBits / 32;
+constexpr int kSubBits = 2048;  // bits per subsequence (one thread)
+constexpr int kWinBits = 512;   // chains are merged within the first kWinBits of a subsequence
+constexpr int kBmWords = kWinBits / 32;
+static_assert(kSubBits == kDecodeSubBits && kThreads == kDecodeBlockSubs && kMaxL == kDecodeMaxL, "decode geometry");
 
 struct DecodeShared {
     u8 fx[kMaxL * kThreads];     // [e][t]: exit offset into the next subsequence or kOOD
     u16 fc[kMaxL * kThreads];    // [e][t]: codewords starting inside
     u32 bm[2 * kBmWords * kThreads];  // [root][word][t]: codeword starts of two root chains
-    u8 sstart[kThreads];
-    u64 scount[kThreads];
+    u64 sstart[kThreads];   // true entry offset of each subsequence (any value)
+    u64 scount[kThreads];   // codewords before it
     u32 slot;
 };
 
@@ -238,6 +240,32 @@ __device__ __forceinline__ void store_sym(void* out, int width, u64 i, u64 v) {
     else static_cast<u64*>(out)[i] = v;
 }
 
+// One-bits of an LSB-first stream from stream position p up to the first zero.
+__device__ __forceinline__ u64 lead_ones(const Stream& s, u64 p) {
+    u64 q = 0;
+    while (p + q < s.total_bits) {
+        const u64 v = peek_lsb64(s.words, s.base + p + q);
+        if (v != ~0ull) return q + (u64)(__ffsll((long long)~v) - 1);
+        q += 64;
+    }
+    return q;
+}
+
+// Entry offsets tracked per subsequence.  Golomb-Rice: a codeword crossing into subsequence s
+// ends at an offset x <= k, or its terminating zero lies inside s after a run of ones that
+// reaches back to s's first bit, so x = k + 1 + (leading ones of s): k + 2 entries, the last
+// one "special".  Other codes: offsets 0 .. L-1.
+template <int KIND>
+__device__ __forceinline__ u32 entry_index(u64 x, int L, int k) {
+    if (KIND == kCodeGolombRice) return x <= (u64)k ? (u32)x : (u32)(k + 1);
+    return x < (u64)L ? (u32)x : kOOD;
+}
+template <int KIND>
+__device__ __forceinline__ u64 entry_offset(const Stream& s, u32 i, u64 Bsub, int k) {
+    if (KIND == kCodeGolombRice && i == (u32)(k + 1)) return (u64)k + 1 + lead_ones(s, Bsub);
+    return i;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -247,7 +275,8 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
     const u64 s = (u64)tile * kThreads + t;
     const u64 first_sub = (u64)tile * kThreads;
     const u32 nvalid = (u32)min((u64)kThreads, a.nsub - first_sub);
-    const int L = a.L_run ? (int)min((u64)kMaxL, (u64)*a.L_run + 1u + (u64)a.s.t.param) : a.L;
+    const int gk = a.s.t.param;
+    const int L = KIND == kCodeGolombRice ? min(kMaxL, gk + 2) : a.L;
     const u64 B = s * kSubBits;
     const u64 Bend = min(B + kSubBits, a.s.total_bits);
 
@@ -256,24 +285,27 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
         u32 rx[2] = {0, 0}, rc[2] = {0, 0};
         int nroots = 0;
         for (int e = 0; e < L; ++e) {
-            u64 p = B + (u64)e;
+            const u64 off = entry_offset<KIND>(a.s, (u32)e, B, gk);
+            u64 p = B + off;
             u32 ox = kOOD, oc = 0;
-            if (p >= Bend) {
-                sh.fx[e * kThreads + t] = (u8)kOOD;
+            if (p >= Bend) {  // no codeword starts here: the entry passes through
+                ox = Bend == B + kSubBits ? entry_index<KIND>(off - kSubBits, L, gk) : kOOD;
+                sh.fx[e * kThreads + t] = (u8)ox;
                 sh.fc[e * kThreads + t] = 0;
                 continue;
             }
             int hit = -1;
-            for (int r = 0; r < nroots; ++r)
-                if (bm_test(sh.bm, r, (u32)e)) hit = r;
+            if (off < (u64)kWinBits)
+                for (int r = 0; r < nroots; ++r)
+                    if (bm_test(sh.bm, r, (u32)off)) hit = r;
             if (hit >= 0) {
                 ox = rx[hit];
-                oc = rc[hit] - bm_popc_below(sh.bm, hit, (u32)e);
+                oc = rc[hit] - bm_popc_below(sh.bm, hit, (u32)off);
             } else {
-                const bool rec = nroots < 2;
+                const bool rec = nroots < 2 && off < (u64)kWinBits;
                 if (rec) {
                     for (int w = 0; w < kBmWords; ++w) sh.bm[(nroots * kBmWords + w) * kThreads + t] = 0;
-                    bm_set(sh.bm, nroots, (u32)e);
+                    bm_set(sh.bm, nroots, (u32)off);
                 }
                 u32 c = 0;
                 bool merged = false;
@@ -281,7 +313,7 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
                     u64 v;
                     p += codeword<KIND>(a.s, p, v);
                     ++c;
-                    if (p < Bend) {
+                    if (p < Bend && p - B < (u64)kWinBits) {
                         const u32 q = (u32)(p - B);
                         for (int r = 0; r < nroots && !merged; ++r)
                             if (bm_test(sh.bm, r, q)) {
@@ -294,8 +326,7 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
                     }
                 }
                 if (!merged) {
-                    const u64 x = p >= B + kSubBits ? p - (B + kSubBits) : (u64)kOOD;
-                    ox = x < (u64)L ? (u32)x : kOOD;
+                    ox = (Bend == B + kSubBits && p >= Bend) ? entry_index<KIND>(p - (B + kSubBits), L, gk) : kOOD;
                     oc = c;
                     if (rec) {
                         rx[nroots] = ox;
@@ -312,6 +343,9 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
 
     // ---- 2. composed table of the block (warp 0; lane holds entries lane and lane+32) ----
     // ---- 3. look-back over predecessor blocks ----
+    // ---- 4. true entry of every subsequence (lane 0 walks the tables; entries outside a
+    //         table, i.e. after a codeword longer than L crossed the boundary, are decoded
+    //         on the spot, so the result is exact for any code) ----
     if (t < 32) {
         u32 gx[2];
         u64 gc[2];
@@ -326,12 +360,12 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
             gx[h] = x;
             gc[h] = c;
         }
-        u32 E = 0;
-        u64 C = 0;
+        u64 E = 0, C = 0;
+        bool failed = false;
         if (tile > 0) {
             for (int h = 0; h < 2; ++h) {
                 const int e = t + 32 * h;
-                if (e < kMaxL) st_volatile(&a.agg[(u64)tile * kMaxL + e], (u64)gx[h] | (gc[h] << 8));
+                st_volatile(&a.agg[(u64)tile * kMaxL + e], (u64)gx[h] | (gc[h] << 8));
             }
             __threadfence();
             __syncwarp();
@@ -341,14 +375,14 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
             u64 Gc[2] = {0, 0};
             long long p = (long long)tile - 1;
             u32 spins = 0;
+            bool need_pred = false;
             while (true) {
                 u32 f = 0;
                 if (t == 0) f = ld_volatile(&a.flag[p]);
                 f = __shfl_sync(kFullMask, f, 0);
                 if (f == 0) {
                     if (++spins > kSpinLimit) {
-                        if (t == 0) atomicOr(a.err, kErrTimeout);
-                        E = kOOD;
+                        failed = true;
                         break;
                     }
                     if (spins > 64) __nanosleep(100);
@@ -356,17 +390,24 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
                 }
                 __threadfence();
                 if (f == 2) {
-                    const u32 X = (u32)ld_volatile(&a.inc[(u64)p * 2]);
+                    const u64 X = ld_volatile(&a.inc[(u64)p * 2]);
                     const u64 CX = ld_volatile(&a.inc[(u64)p * 2 + 1]);
-                    if (X == kOOD) {
-                        E = kOOD;
+                    if (p == (long long)tile - 1) {  // exact entry from the direct predecessor
+                        E = X;
                         C = CX;
                         break;
                     }
-                    const u32 ex0 = __shfl_sync(kFullMask, Gx[0], X & 31u), ex1 = __shfl_sync(kFullMask, Gx[1], X & 31u);
-                    const u64 ec0 = __shfl_sync(kFullMask, Gc[0], X & 31u), ec1 = __shfl_sync(kFullMask, Gc[1], X & 31u);
-                    E = X < 32u ? ex0 : ex1;
-                    C = CX + (X < 32u ? ec0 : ec1);
+                    const u32 Xi = entry_index<KIND>(X, L, gk);
+                    const u32 Xs = Xi == kOOD ? 0u : Xi;
+                    const u32 ex0 = __shfl_sync(kFullMask, Gx[0], Xs & 31u), ex1 = __shfl_sync(kFullMask, Gx[1], Xs & 31u);
+                    const u64 ec0 = __shfl_sync(kFullMask, Gc[0], Xs & 31u), ec1 = __shfl_sync(kFullMask, Gc[1], Xs & 31u);
+                    const u32 gxX = Xs < 32u ? ex0 : ex1;
+                    if (Xi == kOOD || gxX == kOOD) {
+                        need_pred = true;  // the composition does not cover this entry
+                    } else {
+                        E = gxX;
+                        C = CX + (Xs < 32u ? ec0 : ec1);
+                    }
                     break;
                 }
                 // Aggregate F of block p: G <- G o F (both halves read G before either is
@@ -390,47 +431,90 @@ __global__ void __launch_bounds__(kThreads) decode_stream_kernel(DecodeArgs a) {
                 }
                 --p;
                 if (p < 0) {  // cannot happen: tile 0 always publishes its inclusive value
-                    E = kOOD;
+                    failed = true;
                     break;
                 }
             }
+            if (need_pred && !failed) {
+                // Wait for the direct predecessor's exact exit.
+                spins = 0;
+                while (true) {
+                    u32 f = 0;
+                    if (t == 0) f = ld_volatile(&a.flag[tile - 1]);
+                    f = __shfl_sync(kFullMask, f, 0);
+                    if (f == 2u) break;
+                    if (++spins > kSpinLimit) {
+                        failed = true;
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(100);
+                }
+                __threadfence();
+                if (!failed) {
+                    E = ld_volatile(&a.inc[(u64)(tile - 1) * 2]);
+                    C = ld_volatile(&a.inc[(u64)(tile - 1) * 2 + 1]);
+                }
+            }
         }
-        // Own inclusive value: my composed table at entry E.
-        const u32 EE = E == kOOD ? 0u : E;
-        const u32 mx0 = __shfl_sync(kFullMask, gx[0], EE & 31u), mx1 = __shfl_sync(kFullMask, gx[1], EE & 31u);
-        const u64 mc0 = __shfl_sync(kFullMask, gc[0], EE & 31u), mc1 = __shfl_sync(kFullMask, gc[1], EE & 31u);
+        // Fast path: my composed table covers E -> publish my inclusive value right away.
+        // (E is an entry index when it came from a composed table, an offset when it came from
+        // a predecessor's walk; entry_index maps both.)
+        const u32 Ei = entry_index<KIND>(E, L, gk);
+        const u32 Es = Ei == kOOD ? 0u : Ei;
+        const u32 mx0 = __shfl_sync(kFullMask, gx[0], Es & 31u), mx1 = __shfl_sync(kFullMask, gx[1], Es & 31u);
+        const u64 mc0 = __shfl_sync(kFullMask, gc[0], Es & 31u), mc1 = __shfl_sync(kFullMask, gc[1], Es & 31u);
+        const u32 tabX = Es < 32u ? mx0 : mx1;
+        const bool fast = !failed && Ei != kOOD && tabX != kOOD;
         if (t == 0) {
-            const u32 X = E == kOOD ? kOOD : (EE < 32u ? mx0 : mx1);
-            const u64 CC = C + (E == kOOD ? 0ull : (EE < 32u ? mc0 : mc1));
-            st_volatile(&a.inc[(u64)tile * 2], (u64)X);
-            st_volatile(&a.inc[(u64)tile * 2 + 1], CC);
-            __threadfence();
-            st_volatile(&a.flag[tile], 2u);
-            if (E == kOOD) atomicOr(a.need_fallback, 1u);
-            if (tile == gridDim.x - 1) *a.total_codewords = CC;
-            // ---- 4. true entry of each subsequence ----
-            u32 x = E;
+            if (failed) {
+                atomicOr(a.err, kErrTimeout);
+                atomicOr(a.need_fallback, 1u);
+            }
+            if (fast) {
+                st_volatile(&a.inc[(u64)tile * 2], (u64)tabX);
+                st_volatile(&a.inc[(u64)tile * 2 + 1], C + (Es < 32u ? mc0 : mc1));
+                __threadfence();
+                st_volatile(&a.flag[tile], 2u);
+            }
+            // walk my subsequences from the true entry (x: offset into subsequence j)
+            u64 x = E;
+            if (KIND == kCodeGolombRice && E > (u64)gk) x = entry_offset<KIND>(a.s, (u32)(gk + 1), first_sub * kSubBits, gk);
             u64 c = C;
             for (u32 j = 0; j < nvalid; ++j) {
-                sh.sstart[j] = (u8)x;
+                sh.sstart[j] = x;
                 sh.scount[j] = c;
-                if (x == kOOD) continue;
-                c += sh.fc[x * kThreads + j];
-                x = sh.fx[x * kThreads + j];
+                const u32 xi = entry_index<KIND>(x, L, gk);
+                if (xi != kOOD && sh.fx[xi * kThreads + j] != kOOD) {
+                    c += sh.fc[xi * kThreads + j];
+                    const u32 ni = sh.fx[xi * kThreads + j];
+                    x = entry_offset<KIND>(a.s, ni, (first_sub + j + 1) * kSubBits, gk);
+                } else {
+                    const u64 Bj = (first_sub + j) * kSubBits;
+                    const u64 Ej = min(Bj + kSubBits, a.s.total_bits);
+                    u64 pp = Bj + x;
+                    while (pp < Ej) {
+                        u64 v;
+                        pp += codeword<KIND>(a.s, pp, v);
+                        ++c;
+                    }
+                    x = pp >= Bj + kSubBits ? pp - (Bj + kSubBits) : 0ull;
+                }
             }
+            if (!fast) {
+                st_volatile(&a.inc[(u64)tile * 2], x);
+                st_volatile(&a.inc[(u64)tile * 2 + 1], c);
+                __threadfence();
+                st_volatile(&a.flag[tile], 2u);
+            }
+            if (tile == gridDim.x - 1) *a.total_codewords = c;
         }
     }
     __syncthreads();
 
     // ---- 5. decode my subsequence from its true entry ----
     if ((u32)t < nvalid) {
-        const u32 e = sh.sstart[t];
-        if (e == kOOD) {
-            atomicOr(a.need_fallback, 1u);
-            return;
-        }
         u64 idx = sh.scount[t];
-        u64 p = B + e;
+        u64 p = B + sh.sstart[t];
         while (p < Bend && idx < a.nsym) {
             u64 v;
             const u64 len = codeword<KIND>(a.s, p, v);

@@ -170,7 +170,7 @@ struct DecodeTable {
     int zigzag;  // exp-Golomb of a signed symbol type
 };
 constexpr int kDecodeMaxL = 64;       // longest entry offset tracked per subsequence
-constexpr int kDecodeSubBits = 512;   // bits per subsequence (thread)
+constexpr int kDecodeSubBits = 2048;  // bits per subsequence (thread)
 constexpr int kDecodeBlockSubs = 256; // subsequences per thread block
 size_t decode_smem_bytes();
 // flag: [tiles]; agg: [tiles * kDecodeMaxL]; inc: [tiles * 2]; tiles = ceil(ceil(bits/512)/256)
