@@ -9,9 +9,12 @@ copies), Hilbert curve, -rle container, both quantizers (to, cube) x L2 bounds
   value : compress+decompress GB/s (12 bytes per input point) with the points resident in
           HBM, the pre-zstd container produced and consumed in HBM (xnyz_compress_device /
           xnyz_decompress_device), device time from CUDA events on the library's stream.
-  e2e   : the same through the host-buffer C ABI (xnyz_compress / xnyz_decompress): pinned
-          host points in, the reference's zstd level-3 frame out (libzstd 1.5.7 on the host),
-          frame in, host points out; wall clock with device sync on both sides.
+  e2e   : the same through the host-buffer C ABI, batched (xnyz_batch_compress /
+          xnyz_batch_decompress: worker threads with one context each): pinned host points
+          in, the reference's zstd level-3 frames out (libzstd 1.5.7 on the host), frames in,
+          pinned host points out; wall clock with device sync on both sides.  The headline
+          cuts the cloud into --chunk-point pieces, one frame each, exactly the workload the
+          reference arm runs; `monolithic` is one frame per variant for the whole cloud.
   bits/point per variant from the zstd frame.
 
 --gpus N: one process per GPU (torchrun); the path does not shard, every rank runs its
@@ -180,31 +183,55 @@ def run_gpu(args):
     dev_ms = max_over_ranks(dev_ms)
     barrier()
 
-    # ---- end-to-end step through the host-buffer C ABI ----
+    # ---- end-to-end through the host-buffer C ABI: batches of independent calls ----
+    # Pinned host points in, zstd frames out, frames in, pinned host points out; each step
+    # (1) the cloud in `chunk`-point pieces for all variants, the reference arm's per-chunk
+    # workload (headline), and (2) the whole cloud once per variant (one frame each).
+    batch = X.Batch(local, args.workers)
+    host_np = pinned.numpy()
+    outs = [torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy() for _ in variants]
+    bounds = [(a, min(n, a + args.chunk)) for a in range(0, n, args.chunk)]
+    c_clouds = [host_np[a:b] for _ in variants for (a, b) in bounds]
+    c_params = [(q, l2, True, True) for (q, l2) in variants for _ in bounds]
+    c_dparams = [(q, l2, True) for (q, l2) in variants for _ in bounds]
+    c_outs = [outs[vi][a:b] for vi in range(len(variants)) for (a, b) in bounds]
+    m_clouds = [host_np for _ in variants]
+    m_params = [(q, l2, True, True) for (q, l2) in variants]
+    m_dparams = [(q, l2, True) for (q, l2) in variants]
     frame_bytes = {}
-    out_pinned = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+    chunk_bytes = {}
 
-    def e2e_step():
-        for q, l2 in variants:
-            frame = ctx.compress(pinned.numpy(), q, l2, True, True, use_zstd=True)
-            frame_bytes[(q, l2)] = len(frame)
-            out = ctx.decompress(frame, q, l2, True, out=out_pinned)
-            if out.shape[0] != n:
-                raise RuntimeError("e2e decode size mismatch")
+    def e2e_chunked_step():
+        frames = batch.compress(c_clouds, c_params, as_bytes=False)
+        ns = batch.decompress(frames, c_dparams, c_outs)
+        if ns != [b - a for _ in variants for (a, b) in bounds]:
+            raise RuntimeError("e2e (chunked) decode size mismatch")
+        for vi, (q, l2) in enumerate(variants):
+            chunk_bytes[(q, l2)] = sum(len(f) for f in frames[vi * len(bounds):(vi + 1) * len(bounds)])
 
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    for _ in range(min(args.warmup, 1)):
-        e2e_step()
-    barrier()
-    torch.cuda.synchronize(dev)
-    ctx.profile(True)
-    w0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize(dev)
-    e2e_s = max_over_ranks(time.perf_counter() - w0)
-    e2e_prof = {k[5:]: round(v["ms"] / e2e_steps, 2) for k, v in ctx.profile_read().items() if k.startswith("host:")}
-    ctx.profile(False)
+    def e2e_monolithic_step():
+        frames = batch.compress(m_clouds, m_params, as_bytes=False)
+        ns = batch.decompress(frames, m_dparams, outs)
+        if ns != [n] * len(variants):
+            raise RuntimeError("e2e decode size mismatch")
+        for (q, l2), f in zip(variants, frames):
+            frame_bytes[(q, l2)] = len(f)
+
+    def timed(fn, steps):
+        fn()  # warm-up: worker arenas and pinned staging reach their sizes
+        barrier()
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(time.perf_counter() - w0)
+
+    e2e_steps = min(args.steps, args.e2e_steps)  # 0: skip (device-only profiling runs)
+    if e2e_steps:
+        e2e_s = timed(e2e_chunked_step, e2e_steps)
+        mono_s = timed(e2e_monolithic_step, e2e_steps)
+    batch.close()
 
     # ---- CPU baseline: the reference on a bounded sample (rank 0, N = 1) ----
     cpu = None
@@ -214,7 +241,8 @@ def run_gpu(args):
     if rank == 0:
         bytes_step = 12.0 * n * len(variants) * world
         value = bytes_step * args.steps / (dev_ms / 1e3) / 1e9
-        e2e = bytes_step * e2e_steps / e2e_s / 1e9
+        e2e = bytes_step * e2e_steps / e2e_s / 1e9 if e2e_steps else None
+        mono = bytes_step * e2e_steps / mono_s / 1e9 if e2e_steps else None
         peak, peak_kind = load_peaks()
         # dominant kernel: largest total device time among the profiled stages
         dom_name, dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
@@ -224,7 +252,7 @@ def run_gpu(args):
         stage_bytes = sum(v["bytes"] for v in prof.values())
         stage_ms = sum(v["ms"] for v in prof.values())
         launches = sum(v["launches"] for v in prof.values())
-        bpp = {f"{QNAME[q]}_{l2}": round(8.0 * frame_bytes[(q, l2)] / n, 4) for q, l2 in variants}
+        bpp = {f"{QNAME[q]}_{l2}": round(8.0 * frame_bytes[(q, l2)] / n, 4) for q, l2 in variants if (q, l2) in frame_bytes}
         line = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -248,13 +276,23 @@ def run_gpu(args):
                 "direct_threshold": 1024,
                 "l2_flush": "inputs (768 MB per cloud) exceed the 126 MB L2",
                 "value_path": "device-resident points and pre-zstd container",
-                "e2e_path": "host pinned points -> zstd frame -> host points (libzstd 1.5.7 level 3)",
+                "e2e_path": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
+                            "xnyz_batch_compress / xnyz_batch_decompress",
                 "parallelism": f"replicas x{world}",
             },
             "bits_per_point": bpp,
-            "e2e": {"value": round(e2e, 4), "unit": "GB/s", "h2d_bytes_per_step": int(12 * n * len(variants)),
-                    "d2h_bytes_per_step": int(12 * n * len(variants)), "steps": e2e_steps,
-                    "s_per_step": round(e2e_s / e2e_steps, 4), "host_phases_ms_per_step": e2e_prof},
+            "e2e": ({"value": round(e2e, 4), "unit": "GB/s", "h2d_bytes_per_step": int(12 * n * len(variants)),
+                     "d2h_bytes_per_step": int(12 * n * len(variants)), "steps": e2e_steps,
+                     "s_per_step": round(e2e_s / e2e_steps, 4),
+                     "workload": f"{len(bounds)} chunks of {args.chunk} points x {len(variants)} variants "
+                                 f"(the reference arm's per-chunk mode), one zstd frame per chunk, "
+                                 f"xnyz_batch_* with {batch.workers} worker threads",
+                     "bits_per_point": {f"{QNAME[q]}_{l2}": round(8.0 * chunk_bytes[(q, l2)] / n, 4)
+                                        for q, l2 in variants},
+                     "monolithic": {"value": round(mono, 4), "unit": "GB/s", "s_per_step": round(mono_s / e2e_steps, 4),
+                                    "workload": "the whole cloud, one zstd frame per variant, "
+                                                f"{len(variants)} variants in one batch"}}
+                    if e2e_steps else None),
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": None,
@@ -321,7 +359,7 @@ def run_reference(args):
         return
     lib, kind = _ref_lib()
     threads = os.cpu_count() or 1
-    chunk = args.ref_chunk
+    chunk = args.chunk
     n_total = chunk * threads
     host = make_cloud(n_total, 1)
     variants = VARIANTS[: args.variants]
@@ -373,7 +411,8 @@ def main():
     ap.add_argument("--variants", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-points", type=int, default=1_000_000)
-    ap.add_argument("--ref-chunk", type=int, default=150_000)
+    ap.add_argument("--chunk", type=int, default=150_000, help="points per chunk (e2e and the reference arm)")
+    ap.add_argument("--workers", type=int, default=0, help="batch worker threads (0: one per host thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

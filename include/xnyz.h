@@ -149,6 +149,34 @@ xnyz_status xnyz_stage_hilbert(xnyz_ctx* ctx, const uint64_t* dev_in, uint64_t n
  * payload; results replace the inputs. */
 xnyz_status xnyz_stage_sort(xnyz_ctx* ctx, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits);
 
+/* ---- batches of independent clouds ----------------------------------------------------------- */
+
+/* The reference compresses one cloud per call, and a file in chunks (main.cpp:15-71
+ * --offset/--count, one container per chunk; the MPI driver runs chunks in parallel,
+ * mpi_driver.cpp:809-941).  A batch runs many such calls at once: a pool of `workers` host
+ * threads (<= 0: one per hardware thread, at most 32), each with its own context and CUDA
+ * stream on `device`, takes clouds largest first, so the single-threaded libzstd frame of one
+ * cloud overlaps the GPU work and the zstd frames of the others.  Every output is identical
+ * to xnyz_compress / xnyz_decompress_into of that cloud alone. */
+typedef struct xnyz_batch xnyz_batch;
+xnyz_status xnyz_batch_create(xnyz_batch** batch, int device, int workers);
+xnyz_status xnyz_batch_destroy(xnyz_batch* batch);
+int xnyz_batch_workers(const xnyz_batch* batch);
+
+/* Cloud i: xyz[i] (host, or device if xyz_is_device) with n[i] points and params[i].  out[i]
+ * receives a malloc'd frame (release with xnyz_free) of out_len[i] bytes.  item_status (may
+ * be NULL) receives each cloud's status; the return value is the status of the first failing
+ * cloud by index (its message in xnyz_last_error), or XNYZ_OK. */
+xnyz_status xnyz_batch_compress(xnyz_batch* batch, uint64_t count, const float* const* xyz, const uint64_t* n,
+                                int xyz_is_device, const xnyz_params* params, int use_zstd, uint8_t** out,
+                                uint64_t* out_len, xnyz_status* item_status);
+
+/* Frame i: in[i] of in_len[i] bytes, decoded with quantizer[i], l2_bound[i], rle[i] into the
+ * caller's host array xyz[i] of capacity[i] points; n[i] receives the point count. */
+xnyz_status xnyz_batch_decompress(xnyz_batch* batch, uint64_t count, const uint8_t* const* in, const uint64_t* in_len,
+                                  int is_zstd, const int* quantizer, const float* l2_bound, const int* rle,
+                                  float* const* xyz, const uint64_t* capacity, uint64_t* n, xnyz_status* item_status);
+
 /* ---- allocation-free entry point ---------------------------------------------------------- */
 
 /* No counterpart in the reference.  The stable LSD radix sort of xnyz_stage_sort for callers

@@ -16,13 +16,14 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import weakref
 
 import numpy as np
 
 from . import _native as N
 from ._native import CompressInfo, Params, XnyzError
 
-__all__ = ["QUANTIZER_TYPE", "Context", "BlockCompressor", "BlockCompressorRLE", "BlockDecompressor",
+__all__ = ["QUANTIZER_TYPE", "Context", "Batch", "BlockCompressor", "BlockCompressorRLE", "BlockDecompressor",
            "BlockDecompressorRLE", "XnyzError", "CompressInfo", "default_context"]
 
 
@@ -138,6 +139,81 @@ class Context:
         N.check(N.decompress_device(self.handle, C.c_void_p(dev_ptr), length, int(quantizer), float(l2),
                                     int(bool(rle)), C.byref(p), C.byref(n)))
         return p.value, n.value
+
+
+class Batch:
+    """Many independent clouds at once (xnyz_batch_*): a pool of worker threads, each with
+    its own context and stream; outputs are identical to per-cloud Context calls."""
+
+    def __init__(self, device: int = 0, workers: int = 0):
+        h = C.c_void_p()
+        N.check(N.batch_create(C.byref(h), device, int(workers)))
+        self.handle = h
+        self.workers = N.batch_workers(h)
+
+    def close(self):
+        if self.handle:
+            N.batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compress(self, clouds, params, use_zstd: bool = True, item_status: np.ndarray | None = None,
+                 as_bytes: bool = True):
+        """clouds: sequence of (n_i, 3) float32 host arrays; params: sequence of
+        (quantizer, l2, hilbert, rle[, direct_threshold]).  Returns a list of frames: bytes,
+        or (as_bytes=False) uint8 arrays over the library's buffers, freed with the arrays."""
+        k = len(clouds)
+        arrs = [np.ascontiguousarray(c, dtype=np.float32).reshape(-1, 3) for c in clouds]
+        ptrs = (C.c_void_p * k)(*[a.ctypes.data for a in arrs])
+        ns = (C.c_uint64 * k)(*[a.shape[0] for a in arrs])
+        prm = (Params * k)(*[Params(int(p[0]), float(p[1]), int(bool(p[2])), int(bool(p[3])),
+                                    int(p[4]) if len(p) > 4 else 1024) for p in params])
+        outs = (C.c_void_p * k)()
+        lens = (C.c_uint64 * k)()
+        sts = (C.c_int * k)()
+        s = N.batch_compress(self.handle, k, ptrs, ns, 0, prm, int(use_zstd), outs, lens, sts)
+        frames = []
+        for i in range(k):
+            if not outs[i]:
+                frames.append(None)
+            elif as_bytes:
+                frames.append(C.string_at(outs[i], lens[i]))
+                N.free(outs[i])
+            else:
+                buf = (C.c_uint8 * max(1, lens[i])).from_address(outs[i])
+                weakref.finalize(buf, N.free, outs[i])
+                frames.append(np.frombuffer(buf, np.uint8, count=lens[i]))
+        if item_status is not None:
+            item_status[:k] = list(sts)
+        N.check(s)
+        return frames
+
+    def decompress(self, frames, params, outs, is_zstd: bool = True):
+        """frames: sequence of bytes; params: (quantizer, l2, rle) per frame; outs: C-contiguous
+        float32 arrays (e.g. views of pinned memory) receiving the points.  Returns the point
+        counts."""
+        k = len(frames)
+        bufs = [f if isinstance(f, np.ndarray) else np.frombuffer(f, dtype=np.uint8) for f in frames]
+        ins = (C.c_void_p * k)(*[b.ctypes.data for b in bufs])
+        lens = (C.c_uint64 * k)(*[len(f) for f in frames])
+        qs = (C.c_int * k)(*[int(p[0]) for p in params])
+        l2s = (C.c_float * k)(*[float(p[1]) for p in params])
+        rles = (C.c_int * k)(*[int(bool(p[2])) for p in params])
+        os_ = [o.reshape(-1, 3) for o in outs]
+        for o in os_:
+            if o.dtype != np.float32 or not o.flags.c_contiguous:
+                raise ValueError("outputs must be C-contiguous float32 arrays")
+        optr = (C.c_void_p * k)(*[o.ctypes.data for o in os_])
+        caps = (C.c_uint64 * k)(*[o.shape[0] for o in os_])
+        ns = (C.c_uint64 * k)()
+        sts = (C.c_int * k)()
+        N.check(N.batch_decompress(self.handle, k, ins, lens, int(is_zstd), qs, l2s, rles, optr, caps, ns, sts))
+        return list(ns)
 
 
 _default: Context | None = None

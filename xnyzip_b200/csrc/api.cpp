@@ -119,6 +119,12 @@ struct xnyz_ctx {
     uint8_t* d_container = nullptr;  // device container returned by xnyz_compress_device
     size_t d_container_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Side streams for independent streams of one container (the entropy coders and
+    // decoders run concurrently); forked from and joined back into `stream` by events.
+    static constexpr int kSide = 4;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[kSide] = {};
     // stage profiling (xnyz_profile / xnyz_profile_read)
     bool prof = false;
     struct ProfRec {
@@ -174,15 +180,18 @@ struct Prof {
     const char* name;
     uint64_t launches;
     double bytes;
+    cudaStream_t s;
     cudaEvent_t a = nullptr;
-    Prof(xnyz_ctx* cc, const char* nm, uint64_t l, double b) : c(cc), name(nm), launches(l), bytes(b) {
-        if (c->prof && (a = pool_event(c))) cudaEventRecord(a, c->stream);
+    Prof(xnyz_ctx* cc, const char* nm, uint64_t l, double b) : Prof(cc, nm, l, b, cc->stream) {}
+    Prof(xnyz_ctx* cc, const char* nm, uint64_t l, double b, cudaStream_t on)
+        : c(cc), name(nm), launches(l), bytes(b), s(on) {
+        if (c->prof && (a = pool_event(c))) cudaEventRecord(a, s);
     }
     void end() {
         if (!c->prof || !a) return;
         cudaEvent_t e = pool_event(c);
         if (e) {
-            cudaEventRecord(e, c->stream);
+            cudaEventRecord(e, s);
             c->prof_recs.push_back(xnyz_ctx::ProfRec{name, a, e, launches, bytes});
         }
         a = nullptr;
@@ -224,6 +233,22 @@ xnyz_status fetch_small(xnyz_ctx* c, size_t off, size_t bytes) {
     CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c->h_small) + off, reinterpret_cast<char*>(c->d_small) + off,
                              bytes, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return XNYZ_OK;
+}
+
+// Side stream k starts after the work queued so far on the context's stream.
+xnyz_status fork_sides(xnyz_ctx* c) {
+    CUDA_TRY(cudaEventRecord(c->fork_ev, c->stream));
+    for (int k = 0; k < xnyz_ctx::kSide; ++k) CUDA_TRY(cudaStreamWaitEvent(c->side[k], c->fork_ev, 0));
+    return XNYZ_OK;
+}
+
+// The context's stream continues after all work queued on the side streams.
+xnyz_status join_sides(xnyz_ctx* c) {
+    for (int k = 0; k < xnyz_ctx::kSide; ++k) {
+        CUDA_TRY(cudaEventRecord(c->join_ev[k], c->side[k]));
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->join_ev[k], 0));
+    }
     return XNYZ_OK;
 }
 
@@ -728,25 +753,13 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         launch_bitpack(at<unsigned long long>(c, o_dblk), NB, w_blk, at<uint32_t>(c, o_w_blk), st);
         launch_bitpack(at<unsigned long long>(c, o_dcnt), NB, w_cnt, at<uint32_t>(c, o_w_cnt), st);
     }
-    Prof pr_enc(c, "entropy_encode", (P ? 1 : 0) + (code_rep.exp_golomb ? 0 : 1) + (direct ? 0 : 1) + (rle ? 1 : 0),
-                8.0 * P + bits_gr / 8.0 + 2.0 * U + (bits_rep + bits_quad + bits_cnt) / 8.0 + (rle ? 4.0 * U : 0.0));
-    launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
-                     SMALL_FIELD(c, tile_counters[0]),
-                     SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), st);
-    if (!code_rep.exp_golomb)
-        launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
-                              chan(1),
-                              SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err), st);
-    if (!direct)
-        launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
-                              32 * words_for(bits_quad), chan(2),
-                              SMALL_FIELD(c, tile_counters[2]), SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), st);
+    // The four entropy coders are independent: one side stream each.
+    uint32_t* dbits = at<uint32_t>(c, o_dense);
+    uint8_t* dlen = reinterpret_cast<uint8_t*>(dbits + kCountDense);
+    uint32_t* sval = at<uint32_t>(c, o_sparse);
+    uint32_t* sbits = sval + sparse_val.size();
+    uint8_t* slen = reinterpret_cast<uint8_t*>(sbits + sparse_val.size());
     if (rle) {
-        uint32_t* dbits = at<uint32_t>(c, o_dense);
-        uint8_t* dlen = reinterpret_cast<uint8_t*>(dbits + kCountDense);
-        uint32_t* sval = at<uint32_t>(c, o_sparse);
-        uint32_t* sbits = sval + sparse_val.size();
-        uint8_t* slen = reinterpret_cast<uint8_t*>(sbits + sparse_val.size());
         CUDA_TRY(cudaMemcpyAsync(dbits, dense_bits.data(), 4 * kCountDense, cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemcpyAsync(dlen, dense_len.data(), kCountDense, cudaMemcpyHostToDevice, st));
         if (!sparse_val.empty()) {
@@ -754,13 +767,34 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
             CUDA_TRY(cudaMemcpyAsync(sbits, sparse_bits.data(), 4 * sparse_val.size(), cudaMemcpyHostToDevice, st));
             CUDA_TRY(cudaMemcpyAsync(slen, sparse_len.data(), sparse_val.size(), cudaMemcpyHostToDevice, st));
         }
+    }
+    TRY(fork_sides(c));
+    if (P) {
+        Prof pr(c, "encode_golomb_rice", 1, 8.0 * P + bits_gr / 8.0, c->side[0]);
+        launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
+                         SMALL_FIELD(c, tile_counters[0]), SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), c->side[0]);
+    }
+    if (!code_rep.exp_golomb) {
+        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_rep / 8.0, c->side[1]);
+        launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
+                              chan(1), SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err),
+                              c->side[1]);
+    }
+    if (!direct) {
+        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_quad / 8.0, c->side[2]);
+        launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
+                              32 * words_for(bits_quad), chan(2), SMALL_FIELD(c, tile_counters[2]),
+                              SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), c->side[2]);
+    }
+    if (rle) {
+        Prof pr(c, "encode_counts", 1, 4.0 * U + bits_cnt / 8.0, c->side[3]);
         launch_count_encode(at<int32_t>(c, o_counts), U, code_cnt.exp_golomb ? code_cnt.eg_k : -1, dbits, dlen, sval,
                             sbits, slen, static_cast<uint32_t>(sparse_val.size()), at<uint32_t>(c, o_w_cn),
-                            32 * words_for(bits_cnt), chan(3),
-                            SMALL_FIELD(c, tile_counters[3]), SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), st);
+                            32 * words_for(bits_cnt), chan(3), SMALL_FIELD(c, tile_counters[3]),
+                            SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), c->side[3]);
     }
     CUDA_TRY(cudaGetLastError());
-    pr_enc.end();
+    TRY(join_sides(c));
     TRY(fetch_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8));
     TRY(check_device_errors(c));
     const uint64_t gr_bits = c->h_small->totals[0];
@@ -1097,6 +1131,9 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
 
     hd1.end();
     HostPhase hd2(c, "d2_launch");
+    // The entropy-coded streams decode on the side streams while the block streams are
+    // unpacked and scanned on the context's stream.
+    TRY(fork_sides(c));
     // ---- block streams: bit-unpack + prefix sums ----
     if (!h.direct && NB) {
         uint64_t b0, b1;
@@ -1186,18 +1223,20 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                 launch_fill_u32(static_cast<uint32_t*>(j.out), j.nsym, static_cast<uint32_t>(j.fill_value), st);
             continue;
         }
+        cudaStream_t js = c->side[j.slot];
         Prof pr(c, j.kind == kCodeGolombRice ? "decode_golomb_rice" : (j.kind == kCodeHuffman ? "decode_huffman" : "decode_exp_golomb"),
-                1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width);
+                1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width, js);
         // Golomb-Rice tracks k + 2 entry offsets per subsequence (derived in the kernel).
         const uint32_t* Lrun = nullptr;
-        CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_dflag[j.slot]), 0, 4 * dtiles, st));
+        CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_dflag[j.slot]), 0, 4 * dtiles, js));
         launch_decode_stream(j.kind, j.words, j.base_bits, j.total_bits, j.table, j.L, Lrun, j.nsym, j.width, j.out,
                              at<uint32_t>(c, o_dflag[j.slot]), at<unsigned long long>(c, o_dagg[j.slot]),
                              at<unsigned long long>(c, o_dinc[j.slot]), SMALL_FIELD(c, tile_counters[30 + j.slot]),
                              SMALL_FIELD(c, err), SMALL_FIELD(c, fallback[j.slot]), SMALL_FIELD(c, codewords[j.slot]),
-                             st);
+                             js);
     }
     CUDA_TRY(cudaGetLastError());
+    TRY(join_sides(c));
     hd2.end();
     HostPhase hd3(c, "d3_decode_sync");
     // count total (for -rle) after the count stream is decoded
@@ -1308,6 +1347,11 @@ xnyz_status decompress_run(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, con
 
 }  // namespace
 
+namespace xnyz {
+// Sets the calling thread's xnyz_last_error() message (used by the batch pool).
+xnyz_status set_last_error(xnyz_status s, const std::string& msg) { return fail(s, msg); }
+}  // namespace xnyz
+
 // ====================================================================== C ABI ==========
 extern "C" {
 
@@ -1337,6 +1381,11 @@ xnyz_status xnyz_create(xnyz_ctx** out, int device, void* stream) {
     std::memset(c->h_small, 0, sizeof(Small));
     CUDA_TRY(cudaEventCreate(&c->ev0));
     CUDA_TRY(cudaEventCreate(&c->ev1));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    for (int k = 0; k < xnyz_ctx::kSide; ++k) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->join_ev[k], cudaEventDisableTiming));
+    }
     (void)hilbert_machines();
     *out = c.release();
     return XNYZ_OK;
@@ -1355,6 +1404,14 @@ xnyz_status xnyz_destroy(xnyz_ctx* c) {
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (int k = 0; k < xnyz_ctx::kSide; ++k) {
+        if (c->side[k]) {
+            cudaStreamSynchronize(c->side[k]);
+            cudaStreamDestroy(c->side[k]);
+        }
+        if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
+    }
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return XNYZ_OK;
