@@ -940,6 +940,7 @@ struct HuffTables {
     int max_len = 0;
     std::vector<uint32_t> root, tree;
     std::vector<unsigned long long> symvals;
+    bool direct_values = false;  // table payloads are the symbol values (all below 2^24)
 };
 
 xnyz_status build_huff_tables(const ParsedMeta& pm, HuffTables& t) {
@@ -951,6 +952,12 @@ xnyz_status build_huff_tables(const ParsedMeta& pm, HuffTables& t) {
     const int rb = t.root_bits;
     t.root.assign(1u << rb, 0u);
     t.symvals.assign(pm.symbols.begin(), pm.symbols.end());
+    t.direct_values = true;
+    for (unsigned long long v : t.symvals)
+        if (v >= (1ull << 24)) t.direct_values = false;
+    auto payload = [&](size_t oi) {
+        return t.direct_values ? static_cast<uint32_t>(t.symvals[oi]) : static_cast<uint32_t>(oi);
+    };
     // Longer codes first so that a shorter code sharing a prefix wins, as the reference's
     // bit-by-bit matcher stops at the first (shortest) match.
     std::vector<size_t> order(pm.codes.size());
@@ -963,7 +970,7 @@ xnyz_status build_huff_tables(const ParsedMeta& pm, HuffTables& t) {
         const uint32_t bits = len >= 32 ? ce.bits : (ce.bits & ((1u << len) - 1u));
         if (len <= rb) {
             const uint32_t first = bits << (rb - len), span = 1u << (rb - len);
-            for (uint32_t k = 0; k < span; ++k) t.root[first + k] = (static_cast<uint32_t>(len) << 24) | static_cast<uint32_t>(oi);
+            for (uint32_t k = 0; k < span; ++k) t.root[first + k] = (static_cast<uint32_t>(len) << 24) | payload(oi);
         } else {
             const uint32_t top = bits >> (len - rb);
             uint32_t& e = t.root[top];
@@ -997,7 +1004,7 @@ xnyz_status build_huff_tables(const ParsedMeta& pm, HuffTables& t) {
             }
             if (shadowed) continue;
             uint32_t& leaf = t.tree[2 * node + (bits & 1u)];
-            if (leaf == 0xffffffffu) leaf = 0x80000000u | static_cast<uint32_t>(oi);
+            if (leaf == 0xffffffffu) leaf = 0x80000000u | payload(oi);
         }
     }
     if (t.tree.empty()) t.tree.assign(2, 0xffffffffu);
@@ -1176,7 +1183,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         }
         j.table.root = at<uint32_t>(c, o.root);
         j.table.tree = at<uint32_t>(c, o.tree);
-        j.table.symvals = at<unsigned long long>(c, o.sym);
+        j.table.symvals = t.direct_values ? nullptr : at<unsigned long long>(c, o.sym);
         j.table.root_bits = t.root_bits;
         j.L = std::max(1, t.max_len);
         jobs.push_back(j);
@@ -1261,7 +1268,9 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(check_device_errors(c));
     for (auto& j : jobs)
         if (!j.fill && c->h_small->codewords[j.slot] < j.nsym)
-            return fail(XNYZ_ERR_BAD_STREAM, "stream holds fewer codes than points");
+            return fail(XNYZ_ERR_BAD_STREAM, "stream " + std::to_string(j.slot) + " holds " +
+                                                 std::to_string(c->h_small->codewords[j.slot]) + " codes, expected " +
+                                                 std::to_string(j.nsym));
     if (!h.direct && NB && c->h_small->count_total != U)
         return fail(XNYZ_ERR_BAD_STREAM, "block counts do not add up to the point count");
     if (!h.direct && NB == 0 && U) return fail(XNYZ_ERR_BAD_STREAM, "no blocks");

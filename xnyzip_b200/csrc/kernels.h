@@ -155,37 +155,37 @@ void launch_scan_u64(const unsigned long long* in, unsigned long long* out, uint
                      LookBackState lb, uint32_t* tile_counter, unsigned long long* total, uint32_t* err,
                      cudaStream_t st);
 
-// Parallel decoding of one unindexed prefix-code stream (Huffman, Golomb-Rice, exp-Golomb).
+// Parallel decoding of one unindexed prefix-code stream (Huffman, Golomb-Rice, exp-Golomb),
+// implemented in k_stream_decode.cu.
 enum CodeKind { kCodeHuffman = 0, kCodeGolombRice = 1, kCodeExpGolomb = 2 };
 struct DecodeTable {
-    // Huffman: primary table of 2^root_bits entries: (len << 24) | symbol for codes of at
-    // most root_bits bits, 0 for a prefix that is no code, (1u << 31) | node for longer
-    // codes; tree nodes hold two children each (leaf = (1u << 31) | symbol, internal = node
-    // index, missing = 0xffffffff).
+    // Huffman: primary table of 2^root_bits entries (1 <= root_bits <= 11): (len << 24) |
+    // payload for codes of at most root_bits bits, 0 for a prefix that is no code,
+    // (1u << 31) | node for longer codes; tree nodes hold two children each (leaf =
+    // (1u << 31) | payload, internal = node index, missing = 0xffffffff).  The payload is
+    // the symbol value when symvals is null, else an index into symvals.
     const uint32_t* root;
     const uint32_t* tree;
-    const unsigned long long* symvals;  // symbol values; table entries hold indices into it
+    const unsigned long long* symvals;
     int root_bits;
     int param;   // Golomb-Rice / exp-Golomb k
     int zigzag;  // exp-Golomb of a signed symbol type
 };
 constexpr int kDecodeMaxL = 64;       // longest entry offset tracked per subsequence
-constexpr int kDecodeSubBits = 2048;  // bits per subsequence (thread)
-constexpr int kDecodeBlockSubs = 256; // subsequences per thread block
-size_t decode_smem_bytes();
-// flag: [tiles]; agg: [tiles * kDecodeMaxL]; inc: [tiles * 2]; tiles = ceil(ceil(bits/512)/256)
-// The stream starts `base_bits` into `words`.  L = entry offsets tracked (longest codeword);
-// for Golomb-Rice pass L_run (device: longest run of ones) to derive L on the device.
+constexpr int kDecodeSubBits = 512;   // bits per subsequence (thread)
+constexpr int kDecodeBlockSubs = 128; // subsequences per thread block
+// flag: [tiles]; agg: [tiles * kDecodeMaxL]; inc: [tiles * 2];
+// tiles = ceil(ceil(bits / kDecodeSubBits) / kDecodeBlockSubs).
+// The stream starts `base_bits` (< 32) into `words`.  L = entry offsets tracked (the longest
+// codeword; Golomb-Rice derives k + 2 from its parameter, L_run is unused).
 void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t,
                           int L, const uint32_t* L_run, uint64_t nsym, int out_width, void* out, uint32_t* flag,
                           unsigned long long* agg, unsigned long long* inc, uint32_t* tile_counter, uint32_t* err,
                           uint32_t* need_fallback, unsigned long long* total_codewords, cudaStream_t st);
-// One-thread decoder used when a codeword longer than the tracked entry range crosses a
-// subsequence boundary.
+// One-thread decoder the host runs when a bounded wait of the parallel decoder expired.
 void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,
                               DecodeTable t, uint64_t nsym, int out_width, void* out,
                               unsigned long long* total_codewords, uint32_t* err, cudaStream_t st);
-void launch_max_ones_run(const uint32_t* words, uint64_t nwords, uint32_t* out, cudaStream_t st);
 void launch_count_total(const int32_t* counts, uint64_t n, unsigned long long* total, cudaStream_t st);
 void launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cudaStream_t st);
 void launch_fill_u8(uint8_t* p, uint64_t n, uint8_t v, cudaStream_t st);
