@@ -177,6 +177,81 @@ xnyz_status xnyz_batch_decompress(xnyz_batch* batch, uint64_t count, const uint8
                                   int is_zstd, const int* quantizer, const float* l2_bound, const int* rle,
                                   float* const* xyz, const uint64_t* capacity, uint64_t* n, xnyz_status* item_status);
 
+/* ---- extended container: block parameters of the repos / SFC-delta stream ------------------ *
+ * No counterpart in the reference (it codes this stream with one Golomb-Rice k for the
+ * patches and a Huffman code for the PFor symbols, block_compressor.hpp:122-136,174-190).
+ * With a block mode other than XNYZ_BLOCKS_OFF, compress calls on the context write an
+ * extended container: the first 8 bytes are "XNYZBX01", the rest is the reference layout
+ * except that the stream's two entries (Golomb-Rice patches, Huffman symbols) become one
+ * block-coded entry and an empty one.  Each block of 1024 values has its own PFor slot width
+ * w in 0..32 and Golomb-Rice k in 0..31 (escapes, v >= 2^w - 1, hold v - (2^w - 1) as a
+ * Golomb-Rice codeword capped at 96 bits) and its own bit offset, so blocks encode and decode
+ * independently and the decoder never needs the predictor.  Every decompress entry point
+ * recognises the prefix.
+ *   XNYZ_BLOCKS_EXHAUSTIVE  (w, k) minimising each block's size over all 33 x 32 pairs
+ *   XNYZ_BLOCKS_LEARNED     (w, k) predicted by a 34-64-64-(32+33) MLP (BF16 tensor-core
+ *                           layers, FP32 accumulation) from block statistics; blocks whose
+ *                           weaker head has softmax confidence at or below the fallback
+ *                           threshold get the exhaustive search
+ *   XNYZ_BLOCKS_GLOBAL      one pair for all blocks: w = 0, k = floor(log2(mean)) (the plain
+ *                           method's parameter rule, golomb_rice_encoder.hpp:96-104) */
+enum { XNYZ_BLOCKS_OFF = 0, XNYZ_BLOCKS_EXHAUSTIVE = 1, XNYZ_BLOCKS_LEARNED = 2, XNYZ_BLOCKS_GLOBAL = 3 };
+
+typedef struct xnyz_block_info {
+    uint64_t values;           /* values of the block-coded stream (units) */
+    uint64_t blocks;           /* blocks of 1024 values */
+    uint64_t payload_bits;     /* payload size (without the per-block w, k and offsets) */
+    uint64_t fallback_blocks;  /* learned mode: blocks that got the exhaustive search */
+    int mode;                  /* the block mode of the call (0: reference container) */
+} xnyz_block_info;
+
+xnyz_status xnyz_set_block_mode(xnyz_ctx* ctx, int mode);
+/* Predictor parameters (host FP32 array of xnyz_model_param_count() values, the layout the
+ * training entry points use) and the fallback confidence threshold (0: no block falls back,
+ * 1: every block does).
+ * Without a call, learned mode loads model/blockparams.f32 next to the library (or the file
+ * named by XNYZ_MODEL) on first use. */
+xnyz_status xnyz_set_model(xnyz_ctx* ctx, const float* params, uint64_t count, float fallback_confidence);
+uint64_t xnyz_model_param_count(void);
+/* Block statistics of the last compress call on the context. */
+xnyz_status xnyz_last_block_info(xnyz_ctx* ctx, xnyz_block_info* info);
+/* Sets the block mode of every context of a batch. */
+xnyz_status xnyz_batch_set_block_mode(xnyz_batch* batch, int mode);
+
+/* Stage entry points of the block coder and its predictor, for training and tests (device
+ * pointers; `stream` is a cudaStream_t, NULL = default stream; all asynchronous).
+ *   xnyz_stage_repos      the repos / SFC-delta value of every unit in container order (the
+ *                         input of the block coder): runs the compress path on the context and
+ *                         copies min(*count, cap) values to dev_out, *count = number of units
+ *   xnyz_block_features   34 FP32 features per block: fraction of values per
+ *                         min(31, bitlen(v)), mean and max of log2(v + 1) / 64
+ *   xnyz_block_search     exhaustive (w, k) per block and its size in bits (dev_cost may be NULL)
+ *   xnyz_block_cost       size in bits of each block under the given (w, k)
+ *   xnyz_mlp_forward      predictor: argmax w and k per block, the two heads' softmax
+ *                         confidences (dev_conf, 2 per block, may be NULL) and the 65 logits
+ *                         (k logits 0..31, then w logits, may be NULL)
+ *   xnyz_mlp_train_batch  forward + softmax cross-entropy of both heads + backward for samples
+ *                         idx[first .. first + count) (idx NULL: first + i); adds scale * the
+ *                         gradient to dev_grad and scale * the summed loss to dev_loss;
+ *                         dev_gather is scratch of xnyz_mlp_gather_floats(count) floats
+ *   xnyz_mlp_adam         Adam step (beta 0.9 / 0.999, eps 1e-8, step counted from 1) that also
+ *                         clears dev_grad */
+xnyz_status xnyz_stage_repos(xnyz_ctx* ctx, const float* dev_xyz, uint64_t n, const xnyz_params* params,
+                             uint64_t* dev_out, uint64_t cap, uint64_t* count);
+xnyz_status xnyz_block_features(const uint64_t* dev_vals, uint64_t n, float* dev_feats, void* stream);
+xnyz_status xnyz_block_search(const uint64_t* dev_vals, uint64_t n, uint8_t* dev_w, uint8_t* dev_k,
+                              uint32_t* dev_cost, void* stream);
+xnyz_status xnyz_block_cost(const uint64_t* dev_vals, uint64_t n, const uint8_t* dev_w, const uint8_t* dev_k,
+                            uint32_t* dev_cost, void* stream);
+xnyz_status xnyz_mlp_forward(const float* dev_params, const float* dev_feats, uint64_t count, uint8_t* dev_w,
+                             uint8_t* dev_k, float* dev_conf, float* dev_logits, void* stream);
+uint64_t xnyz_mlp_gather_floats(uint64_t count);
+xnyz_status xnyz_mlp_train_batch(const float* dev_params, const float* dev_feats, const uint8_t* dev_w,
+                                 const uint8_t* dev_k, const uint32_t* dev_idx, uint64_t first, uint64_t count,
+                                 float scale, float* dev_grad, float* dev_loss, float* dev_gather, void* stream);
+xnyz_status xnyz_mlp_adam(float* dev_params, float* dev_grad, float* dev_m, float* dev_v, float lr, int step,
+                          void* stream);
+
 /* ---- allocation-free entry point ---------------------------------------------------------- */
 
 /* No counterpart in the reference.  The stable LSD radix sort of xnyz_stage_sort for callers

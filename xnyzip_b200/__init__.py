@@ -132,6 +132,29 @@ class Context:
         self.last_info = info
         return p.value, ln.value
 
+    # -- extended container (block parameters of the repos / SFC-delta stream) ---------
+    def set_block_mode(self, mode: int):
+        """0 reference container, 1 exhaustive, 2 learned, 3 one global pair (N.BLOCKS_*)."""
+        N.check(N.set_block_mode(self.handle, int(mode)))
+
+    def set_model(self, params: np.ndarray, fallback_confidence: float = 0.5):
+        prm = np.ascontiguousarray(params, dtype=np.float32).ravel()
+        N.check(N.set_model(self.handle, prm.ctypes.data_as(C.c_void_p), prm.size, float(fallback_confidence)))
+
+    def block_info(self) -> dict:
+        bi = N.BlockInfo()
+        N.check(N.last_block_info(self.handle, C.byref(bi)))
+        return bi.as_dict()
+
+    def stage_repos(self, dev_ptr: int, n: int, quantizer: int, l2: float, hilbert: bool, rle: bool, out_ptr: int,
+                    cap: int, direct_threshold: int = 1024) -> int:
+        """Repos / SFC-delta value of every unit (device u64 array at out_ptr); returns the count."""
+        prm = Params(int(quantizer), float(l2), int(bool(hilbert)), int(bool(rle)), int(direct_threshold))
+        cnt = C.c_uint64()
+        N.check(N.stage_repos(self.handle, C.c_void_p(dev_ptr), n, C.byref(prm), C.c_void_p(out_ptr), cap,
+                              C.byref(cnt)))
+        return cnt.value
+
     def decompress_device(self, dev_ptr: int, length: int, quantizer: int, l2: float, rle: bool):
         """Device container -> (device pointer to 3*n floats owned by the context, n)."""
         p = C.c_void_p()

@@ -93,6 +93,32 @@ host_hilbert = _proto("xnyz_host_hilbert", [_p, C.c_uint64, C.c_uint, C.c_int, _
 host_codebook = _proto("xnyz_host_codebook", [C.c_int, C.c_int, _p, _p, _p, C.c_uint64, C.c_uint64, _p,
                                               C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_int)])
 
+class BlockInfo(C.Structure):
+    _fields_ = [("values", C.c_uint64), ("blocks", C.c_uint64), ("payload_bits", C.c_uint64),
+                ("fallback_blocks", C.c_uint64), ("mode", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+set_block_mode = _proto("xnyz_set_block_mode", [_p, C.c_int])
+set_model = _proto("xnyz_set_model", [_p, _p, C.c_uint64, C.c_float])
+model_param_count = _proto("xnyz_model_param_count", [], C.c_uint64)
+last_block_info = _proto("xnyz_last_block_info", [_p, C.POINTER(BlockInfo)])
+batch_set_block_mode = _proto("xnyz_batch_set_block_mode", [_p, C.c_int])
+stage_repos = _proto("xnyz_stage_repos", [_p, _p, C.c_uint64, C.POINTER(Params), _p, C.c_uint64,
+                                          C.POINTER(C.c_uint64)])
+block_features = _proto("xnyz_block_features", [_p, C.c_uint64, _p, _p])
+block_search = _proto("xnyz_block_search", [_p, C.c_uint64, _p, _p, _p, _p])
+block_cost = _proto("xnyz_block_cost", [_p, C.c_uint64, _p, _p, _p, _p])
+mlp_forward = _proto("xnyz_mlp_forward", [_p, _p, C.c_uint64, _p, _p, _p, _p, _p])
+mlp_gather_floats = _proto("xnyz_mlp_gather_floats", [C.c_uint64], C.c_uint64)
+mlp_train_batch = _proto("xnyz_mlp_train_batch", [_p, _p, _p, _p, _p, C.c_uint64, C.c_uint64, C.c_float, _p, _p, _p,
+                                                  _p])
+mlp_adam = _proto("xnyz_mlp_adam", [_p, _p, _p, _p, C.c_float, C.c_int, _p])
+
+BLOCKS_OFF, BLOCKS_EXHAUSTIVE, BLOCKS_LEARNED, BLOCKS_GLOBAL = 0, 1, 2, 3
+
 # Every symbol include/xnyz.h declares (checked by the tests).
 EXPORTED = [
     "xnyz_create", "xnyz_destroy", "xnyz_last_error", "xnyz_version", "xnyz_set_zstd_library", "xnyz_host_alloc",
@@ -100,6 +126,9 @@ EXPORTED = [
     "xnyz_decompress_device", "xnyz_free", "xnyz_stage_quantize", "xnyz_stage_recover", "xnyz_stage_hilbert",
     "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_sort_noalloc", "xnyz_decompress_into",
     "xnyz_batch_create", "xnyz_batch_destroy", "xnyz_batch_workers", "xnyz_batch_compress", "xnyz_batch_decompress",
+    "xnyz_set_block_mode", "xnyz_set_model", "xnyz_model_param_count", "xnyz_last_block_info",
+    "xnyz_batch_set_block_mode", "xnyz_stage_repos", "xnyz_block_features", "xnyz_block_search", "xnyz_block_cost",
+    "xnyz_mlp_forward", "xnyz_mlp_gather_floats", "xnyz_mlp_train_batch", "xnyz_mlp_adam",
 ]
 
 

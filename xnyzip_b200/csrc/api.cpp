@@ -10,6 +10,7 @@
 //   -> bit-unpack + prefix sums -> parallel Golomb-Rice / Huffman / exp-Golomb decoding
 //   -> fused LCP recovery, PFor decode, expansion, recover and unshift.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <chrono>
@@ -57,6 +58,9 @@ xnyz_status fail(xnyz_status s, const std::string& msg) {
     } while (0)
 
 constexpr size_t kAlign = 256;
+// First 8 bytes of an extended container ("XNYZBX01"): the reference container follows,
+// except that the repos / SFC-delta stream is block-coded (k_blocks.cu).
+constexpr uint64_t kExtMagic = 0x313058425a594e58ull;
 inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
 inline uint64_t cdiv(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline int bitlen(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
@@ -79,6 +83,9 @@ struct Small {
     unsigned long long totals[8];
     unsigned long long codewords[8];
     unsigned long long count_total;
+    unsigned long long ext_bits;      // extended container: block payload bits
+    unsigned long long ext_fallback;  // extended container: blocks searched exhaustively
+    double ext_sum;                   // extended container: sum of the stream (global mode)
     uint32_t tile_counters[64];
     uint32_t sort_hist[8 * 256];
     ByteCodes codes[2];
@@ -137,6 +144,13 @@ struct xnyz_ctx {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::map<std::string, std::pair<double, uint64_t>> host_ms;  // host phase wall time, calls
+    // extended container (block parameters of the repos / SFC-delta stream)
+    int block_mode = XNYZ_BLOCKS_OFF;
+    float* d_model = nullptr;      // predictor parameters (kParamCount FP32)
+    float fallback_conf = 0.5f;    // learned mode: blocks below this confidence are searched
+    xnyz_block_info last_blocks{};
+    const unsigned long long* last_repval = nullptr;  // rep values of the last extended compress
+    uint64_t last_repval_n = 0;
 };
 
 namespace {
@@ -360,6 +374,24 @@ struct Container {
             size += data_bytes;
         }
     }
+    // A stream whose data is several parts: device memory, or zero bytes where ptr is null.
+    void stream_parts(const std::vector<uint8_t>& meta, std::initializer_list<std::pair<const void*, size_t>> parts) {
+        size_t total = 0;
+        for (const auto& pr : parts) total += pr.second;
+        pod<uint64_t>(total);
+        pod<uint64_t>(meta.size());
+        host_bytes(meta.data(), meta.size());
+        for (const auto& pr : parts) {
+            if (!pr.second) continue;
+            if (pr.first) {
+                pieces.push_back(Piece{size, pr.second, 0, pr.first});
+                size += pr.second;
+            } else {
+                const std::vector<uint8_t> z(pr.second, 0);
+                host_bytes(z.data(), z.size());
+            }
+        }
+    }
     // Assemble into host memory (device pieces copied asynchronously on `st`).
     cudaError_t to_host(uint8_t* dst, cudaStream_t st) const {
         for (const Piece& pc : pieces) {
@@ -423,9 +455,10 @@ struct CPlan {
     size_t o_k0, o_k1, o_v0, o_v1, o_rep, o_quad, o_patch, o_blkid, o_blkunit, o_unitpos, o_counts, o_over_v,
         o_over_u, o_dblk, o_dcnt;
     LB lb_units, lb_enc;
+    size_t o_repval = 0, o_xw = 0, o_xk = 0, o_xoff = 0, o_xcost = 0, o_xfeat = 0, o_xconf = 0, o_xflag = 0;
     size_t total;
 };
-CPlan make_cplan(uint64_t n, bool want_order, size_t reserved) {
+CPlan make_cplan(uint64_t n, bool want_order, size_t reserved, bool ext) {
     CPlan c{};
     c.tiles = cdiv(n, kSortTile);
     Plan pl;
@@ -447,11 +480,87 @@ CPlan make_cplan(uint64_t n, bool want_order, size_t reserved) {
     c.o_dcnt = pl.add(8 * n);
     c.lb_units = plan_lb(pl, c.tiles, 3);
     c.lb_enc = plan_lb(pl, c.tiles, 4);
+    if (ext) {
+        const uint64_t nb = cdiv(n, kParamBlock);
+        c.o_repval = pl.add(8 * n);
+        c.o_xw = pl.add(nb);
+        c.o_xk = pl.add(nb);
+        c.o_xoff = pl.add(8 * nb);
+        c.o_xcost = pl.add(4 * nb);
+        c.o_xfeat = pl.add(4ull * kParamFeatures * nb);
+        c.o_xconf = pl.add(8 * nb);
+        c.o_xflag = pl.add(nb);
+    }
     c.total = pl.total;
     return c;
 }
 // Typical encoder output space (grown on demand when a stream is larger).
 size_t encoder_reserve(uint64_t n) { return 4 * n + (8u << 20); }
+
+// Loads the predictor shipped next to the library (model/blockparams.f32) unless one is set.
+xnyz_status ensure_model(xnyz_ctx* c) {
+    if (c->d_model) return XNYZ_OK;
+    Dl_info di{};
+    std::string path;
+    if (const char* env = std::getenv("XNYZ_MODEL")) {
+        path = env;
+    } else if (dladdr(reinterpret_cast<void*>(&ensure_model), &di) && di.dli_fname) {
+        path = di.dli_fname;
+        const size_t slash = path.rfind('/');
+        path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/model/blockparams.f32";
+    }
+    std::vector<float> prm(kParamCount);
+    FILE* f = path.empty() ? nullptr : std::fopen(path.c_str(), "rb");
+    if (!f) return fail(XNYZ_ERR_INVALID_ARG, "no block-parameter model: call xnyz_set_model (looked for " + path + ")");
+    const size_t got = std::fread(prm.data(), sizeof(float), prm.size(), f);
+    std::fclose(f);
+    if (got != prm.size()) return fail(XNYZ_ERR_INVALID_ARG, "block-parameter model file has the wrong size: " + path);
+    CUDA_TRY(cudaMalloc(&c->d_model, sizeof(float) * kParamCount));
+    CUDA_TRY(cudaMemcpy(c->d_model, prm.data(), sizeof(float) * kParamCount, cudaMemcpyHostToDevice));
+    return XNYZ_OK;
+}
+
+// Chooses (w, k) per 1024-value block of the repos / SFC-delta values (cp.o_repval) by the
+// context's block mode, then the block sizes and offsets (payload bits in Small::ext_bits).
+xnyz_status select_block_params(xnyz_ctx* c, const CPlan& cp, uint64_t U, uint64_t nb) {
+    cudaStream_t st = c->stream;
+    TRY(memset_small(c, offsetof(Small, ext_bits), 3 * sizeof(unsigned long long), 0));
+    if (!U) return XNYZ_OK;
+    const unsigned long long* rv = at<unsigned long long>(c, cp.o_repval);
+    uint8_t* xw = at<uint8_t>(c, cp.o_xw);
+    uint8_t* xk = at<uint8_t>(c, cp.o_xk);
+    uint32_t* xcost = at<uint32_t>(c, cp.o_xcost);
+    if (c->block_mode == XNYZ_BLOCKS_LEARNED) {
+        TRY(ensure_model(c));
+        float* feats = at<float>(c, cp.o_xfeat);
+        float* conf = at<float>(c, cp.o_xconf);
+        uint8_t* flags = at<uint8_t>(c, cp.o_xflag);
+        {
+            Prof pr(c, "block_features", 1, 8.0 * U + 4.0 * kParamFeatures * nb);
+            launch_block_features(rv, U, feats, st);
+        }
+        {
+            Prof pr(c, "mlp_forward", 1, 4.0 * kParamFeatures * nb + 10.0 * nb);
+            launch_mlp_forward(c->d_model, feats, nb, xw, xk, conf, nullptr, st);
+            launch_block_fallback(conf, nb, c->fallback_conf, flags, SMALL_FIELD(c, ext_fallback), st);
+        }
+        Prof pr(c, "block_search", 1, 8.0 * U);
+        launch_block_search(rv, U, flags, xw, xk, nullptr, st);
+    } else if (c->block_mode == XNYZ_BLOCKS_EXHAUSTIVE) {
+        Prof pr(c, "block_search", 1, 8.0 * U);
+        launch_block_search(rv, U, nullptr, xw, xk, nullptr, st);
+    } else {
+        Prof pr(c, "block_global", 2, 8.0 * U);
+        launch_block_global(rv, U, SMALL_FIELD(c, ext_sum), xw, xk, st);
+    }
+    {
+        Prof pr(c, "block_cost", 2, 8.0 * U + 12.0 * nb);
+        launch_block_cost(rv, U, xw, xk, xcost, st);
+        launch_block_offsets(xcost, nb, at<unsigned long long>(c, cp.o_xoff), SMALL_FIELD(c, ext_bits), st);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
 
 xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& prm, bool want_order,
                           size_t arena_reserved, CompressOut& R) {
@@ -546,7 +655,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     const int passes = static_cast<int>(cdiv(key_bits, 8));
 
     // ---- 3. arena plan ----
-    const CPlan cp = make_cplan(n, want_order, arena_reserved);
+    const bool ext = c->block_mode != XNYZ_BLOCKS_OFF;
+    const CPlan cp = make_cplan(n, want_order, arena_reserved, ext);
     const uint64_t tiles = cp.tiles;
     const size_t o_k0 = cp.o_k0, o_k1 = cp.o_k1, o_v0 = cp.o_v0, o_v1 = cp.o_v1, o_rep = cp.o_rep, o_quad = cp.o_quad,
                  o_patch = cp.o_patch, o_blkid = cp.o_blkid, o_blkunit = cp.o_blkunit, o_unitpos = cp.o_unitpos,
@@ -586,7 +696,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     TRY(memset_small(c, offsetof(Small, first_quad), sizeof(uint32_t) * 256, 0xff));
     TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 64, 0));
     TRY(lb_clear(c, lb_units, 3));
-    UnitOutputs uo;
+    UnitOutputs uo{};
+    uo.rep_val = ext ? at<unsigned long long>(c, cp.o_repval) : nullptr;
     uo.rep_sym = at<uint8_t>(c, o_rep);
     uo.quad_sym = at<uint8_t>(c, o_quad);
     uo.patches = at<unsigned long long>(c, o_patch);
@@ -631,6 +742,9 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         launch_block_deltas(uo.blk_id, uo.blk_unit, NB, U, at<unsigned long long>(c, o_dblk),
                             at<unsigned long long>(c, o_dcnt), c->d_small->max2, st);
     }
+    // ---- 6b. extended container: block parameters of the repos / SFC-delta stream ----
+    const uint64_t ext_nb = ext ? cdiv(U, kParamBlock) : 0;
+    if (ext) TRY(select_block_params(c, cp, U, ext_nb));
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, hist_rep),
                     offsetof(Small, tile_counters) - offsetof(Small, hist_rep)));  // hists, counts, maxima
@@ -645,7 +759,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         if (!direct && H.hist_quad[s])
             st_quad.push_back(SymbolStat{static_cast<uint64_t>(s), H.hist_quad[s], H.first_quad[s]});
     }
-    const StreamCode code_rep = build_stream_code(SymType::U64, st_rep, U);
+    const StreamCode code_rep = ext ? StreamCode{} : build_stream_code(SymType::U64, st_rep, U);
     StreamCode code_quad;
     if (!direct) code_quad = build_stream_code(SymType::U8, st_quad, U);
     StreamCode code_cnt;
@@ -719,10 +833,12 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     // bounded by P*(k+1) + sum(v >> k) <= P*(k+1) + (sum >> k) + P.
     const uint64_t bits_rep = code_rep.encoded_bits, bits_quad = direct ? 0 : code_quad.encoded_bits;
     const uint64_t bits_cnt = rle ? code_cnt.encoded_bits : 0;
-    const unsigned __int128 gr_bound = static_cast<unsigned __int128>(P) * (grk + 2) + (psum >> grk);
+    const unsigned __int128 gr_bound =
+        ext ? 0 : static_cast<unsigned __int128>(P) * (grk + 2) + (psum >> grk);
     if (gr_bound > (static_cast<unsigned __int128>(1) << 40))
         return fail(XNYZ_ERR_UNSUPPORTED, "Golomb-Rice stream larger than 2^40 bits");
     const uint64_t bits_gr = static_cast<uint64_t>(gr_bound);
+    const uint64_t ext_bits = ext ? H.ext_bits : 0;
     auto words_for = [](uint64_t bits) { return cdiv(bits, 32) + 4; };
     Plan pe;
     pe.total = pl.total;
@@ -734,6 +850,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     const size_t o_w_cn = pe.add(4 * words_for(bits_cnt));
     const size_t o_dense = pe.add(kCountDense * 5);
     const size_t o_sparse = pe.add(sparse_val.size() * 9 + 16);
+    const size_t o_w_xp = pe.add(4 * words_for(ext_bits));
     const size_t enc_begin = o_w_blk, enc_end = pe.total;
     if (pe.total > c->arena.cap) {
         // Growing would move the arena; the inputs above live in it.  Plan for the worst
@@ -769,12 +886,17 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         }
     }
     TRY(fork_sides(c));
-    if (P) {
+    if (ext && U) {
+        Prof pr(c, "encode_blocks", 1, 8.0 * U + ext_bits / 8.0, c->side[0]);
+        launch_block_encode(at<unsigned long long>(c, cp.o_repval), U, at<uint8_t>(c, cp.o_xw), at<uint8_t>(c, cp.o_xk),
+                            at<unsigned long long>(c, cp.o_xoff), at<uint32_t>(c, o_w_xp), c->side[0]);
+    }
+    if (P && !ext) {
         Prof pr(c, "encode_golomb_rice", 1, 8.0 * P + bits_gr / 8.0, c->side[0]);
         launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
                          SMALL_FIELD(c, tile_counters[0]), SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), c->side[0]);
     }
-    if (!code_rep.exp_golomb) {
+    if (!ext && !code_rep.exp_golomb) {
         Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_rep / 8.0, c->side[1]);
         launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
                               chan(1), SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err),
@@ -798,7 +920,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     TRY(fetch_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8));
     TRY(check_device_errors(c));
     const uint64_t gr_bits = c->h_small->totals[0];
-    if (!code_rep.exp_golomb && c->h_small->totals[1] != bits_rep)
+    if (!ext && !code_rep.exp_golomb && c->h_small->totals[1] != bits_rep)
         return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (repos)");
     if (!direct && c->h_small->totals[2] != bits_quad) return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (quads)");
     if (rle && c->h_small->totals[3] != bits_cnt) return fail(XNYZ_ERR_CUDA, "count encoder size mismatch");
@@ -807,6 +929,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     HostPhase hp6(c, "c6_container");
     // ---- 9. container (Appendix: block_compressor.hpp:56-215, block_compressor_rle.hpp:125-314) ----
     Container& K = R.cont;
+    if (ext) K.pod<uint64_t>(kExtMagic);
     K.pod<uint64_t>(U);
     K.pod<uint64_t>(0);  // params.size(): the cube and truncated-octahedron quantizers have none
     K.pod<int32_t>(rx);
@@ -815,16 +938,32 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     K.pod<uint8_t>(hil ? 1 : 0);
     K.pod<uint8_t>(direct ? 1 : 0);
     const std::vector<uint8_t> gr_meta = P ? le5(static_cast<uint32_t>(P), grk) : std::vector<uint8_t>{};
+    // the repos / SFC-delta stream: GR(patches) + Huffman(PFor symbols), or the block stream
+    auto rep_streams = [&]() {
+        if (ext) {
+            std::vector<uint8_t> meta(16);
+            std::memcpy(meta.data(), &U, 8);
+            std::memcpy(meta.data() + 8, &ext_bits, 8);
+            const size_t pad = (8 - (2 * ext_nb) % 8) % 8;
+            K.stream_parts(meta, {{at<uint8_t>(c, cp.o_xw), ext_nb},
+                                  {at<uint8_t>(c, cp.o_xk), ext_nb},
+                                  {nullptr, pad},
+                                  {at<unsigned long long>(c, cp.o_xoff), 8 * ext_nb},
+                                  {at<uint32_t>(c, o_w_xp), cdiv(ext_bits, 8)}});
+            K.stream({}, nullptr, 0);
+        } else {
+            K.stream(gr_meta, at<uint32_t>(c, o_w_gr), P ? cdiv(gr_bits, 8) : 0);
+            K.stream(code_rep.meta, at<uint32_t>(c, o_w_rep), cdiv(bits_rep, 8));
+        }
+    };
     if (direct) {
-        K.stream(gr_meta, at<uint32_t>(c, o_w_gr), P ? cdiv(gr_bits, 8) : 0);
-        K.stream(code_rep.meta, at<uint32_t>(c, o_w_rep), cdiv(bits_rep, 8));
+        rep_streams();
     } else {
         K.stream(le5(static_cast<uint32_t>(NB), static_cast<uint8_t>(w_blk)), at<uint32_t>(c, o_w_blk),
                  cdiv(NB * static_cast<uint64_t>(w_blk), 8));
         K.stream(le5(static_cast<uint32_t>(NB), static_cast<uint8_t>(w_cnt)), at<uint32_t>(c, o_w_cnt),
                  cdiv(NB * static_cast<uint64_t>(w_cnt), 8));
-        K.stream(gr_meta, at<uint32_t>(c, o_w_gr), P ? cdiv(gr_bits, 8) : 0);
-        K.stream(code_rep.meta, at<uint32_t>(c, o_w_rep), cdiv(bits_rep, 8));
+        rep_streams();
         K.stream({}, nullptr, 0);  // quad patches: quad deltas are < 8, never patched
         K.stream(code_quad.meta, at<uint32_t>(c, o_w_quad), cdiv(bits_quad, 8));
     }
@@ -848,6 +987,16 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     std::memcpy(&emax, &S.mse_max_bits, 4);
     I.max_l2_error = std::sqrt(static_cast<double>(emax));
     I.mse = S.mse_sum / static_cast<double>(n);
+    c->last_blocks = xnyz_block_info{};
+    c->last_repval = ext ? at<unsigned long long>(c, cp.o_repval) : nullptr;
+    c->last_repval_n = ext ? U : 0;
+    if (ext) {
+        c->last_blocks.values = U;
+        c->last_blocks.blocks = ext_nb;
+        c->last_blocks.payload_bits = ext_bits;
+        c->last_blocks.fallback_blocks = H.ext_fallback;
+        c->last_blocks.mode = c->block_mode;
+    }
     return XNYZ_OK;
 }
 
@@ -885,6 +1034,7 @@ struct StreamRef {
     std::vector<uint8_t> meta;
 };
 struct Header {
+    bool ext = false;  // extended container (block-coded repos / SFC-delta stream)
     uint64_t units = 0;
     int32_t rx = 0, ry = 0, rz = 0;
     bool hilbert = false, direct = false;
@@ -905,7 +1055,12 @@ xnyz_status parse_header(Read rd, uint64_t len, bool rle, Header& h) {
     };
     uint64_t np = 0;
     uint8_t hb = 0, db = 0;
-    if (!get(&h.units, 8) || !get(&np, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    if (!get(&h.units, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    if (h.units == kExtMagic) {
+        h.ext = true;
+        if (!get(&h.units, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    }
+    if (!get(&np, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
     if (np > (len - p) / 4) return fail(XNYZ_ERR_BAD_STREAM, "bad parameter count");
     p += 4 * np;  // quantizer parameters (none for cube / truncated octahedron)
     if (!get(&h.rx, 4) || !get(&h.ry, 4) || !get(&h.rz, 4) || !get(&hb, 1) || !get(&db, 1))
@@ -1043,7 +1198,20 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     const StreamRef& s_sym = h.streams[i_sym];
     uint64_t P = 0;
     uint8_t grk = 0;
-    if (!(s_gr.meta.empty() && s_gr.data_len == 0)) {
+    // extended container: the block-coded stream in the Golomb-Rice slot, the symbol slot empty
+    uint64_t x_nb = 0, x_bits = 0;
+    if (h.ext) {
+        if (s_gr.meta.size() != 16 || !s_sym.meta.empty() || s_sym.data_len)
+            return fail(XNYZ_ERR_BAD_STREAM, "malformed block-coded stream");
+        uint64_t nv = 0;
+        std::memcpy(&nv, s_gr.meta.data(), 8);
+        std::memcpy(&x_bits, s_gr.meta.data() + 8, 8);
+        if (nv != U) return fail(XNYZ_ERR_BAD_STREAM, "block-coded stream and point count disagree");
+        x_nb = cdiv(U, kParamBlock);
+        const uint64_t pad = (8 - (2 * x_nb) % 8) % 8;
+        if (x_bits > (1ull << 50) || s_gr.data_len != 2 * x_nb + pad + 8 * x_nb + cdiv(x_bits, 8))
+            return fail(XNYZ_ERR_BAD_STREAM, "block-coded stream has the wrong size");
+    } else if (!(s_gr.meta.empty() && s_gr.data_len == 0)) {
         if (s_gr.meta.size() != 5) return fail(XNYZ_ERR_BAD_STREAM, "Invalid meta size in Golomb-Rice packed data");
         P = le32(s_gr.meta);
         grk = s_gr.meta[4];
@@ -1051,7 +1219,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     }
     std::string perr;
     ParsedMeta pm_sym, pm_quad, pm_cnt;
-    if (!parse_meta(SymType::U64, s_sym.meta.data(), s_sym.meta.size(), pm_sym, perr))
+    if (!h.ext && !parse_meta(SymType::U64, s_sym.meta.data(), s_sym.meta.size(), pm_sym, perr))
         return fail(XNYZ_ERR_BAD_STREAM, perr);
     uint64_t NB = 0;
     int w_blk = 0, w_cnt = 0;
@@ -1090,12 +1258,14 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     const size_t o_patch = pl.add(8 * P + 8);
     const size_t o_rep = pl.add(U + 8), o_quad = pl.add(U + 8), o_isst = pl.add(U + 8), o_stb = pl.add(4 * U + 8);
     const size_t o_counts = pl.add(4 * U + 8);
+    const size_t o_xw = h.ext ? pl.add(x_nb) : 0, o_xk = h.ext ? pl.add(x_nb) : 0, o_xoff = h.ext ? pl.add(8 * x_nb) : 0,
+                 o_xpay = h.ext ? pl.add(4 * (cdiv(x_bits, 32) + 2)) : 0, o_rv = h.ext ? pl.add(8 * U + 8) : 0;
     const LB lb_scan = plan_lb(pl, cdiv(std::max<uint64_t>(NB, 1), kScanTile), 3);
     struct TabOff {
         size_t root, tree, sym;
     };
     HuffTables ht_sym, ht_quad, ht_cnt;
-    TRY(build_huff_tables(pm_sym, ht_sym));
+    if (!h.ext) TRY(build_huff_tables(pm_sym, ht_sym));
     if (!h.direct) TRY(build_huff_tables(pm_quad, ht_quad));
     if (rle && !pm_cnt.exp_golomb) TRY(build_huff_tables(pm_cnt, ht_cnt));
     auto plan_tab = [&](const HuffTables& t) {
@@ -1202,7 +1372,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         j.L = -1;  // from the longest one-run
         jobs.push_back(j);
     }
-    TRY(huff_job(s_sym, pm_sym, ht_sym, to_sym, 1, at<uint8_t>(c, o_rep), 1));
+    if (!h.ext) TRY(huff_job(s_sym, pm_sym, ht_sym, to_sym, 1, at<uint8_t>(c, o_rep), 1));
     if (!h.direct) TRY(huff_job(h.streams[5], pm_quad, ht_quad, to_quad, 1, at<uint8_t>(c, o_quad), 2));
     if (rle) {
         if (pm_cnt.exp_golomb) {
@@ -1221,6 +1391,22 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         } else {
             TRY(huff_job(*s_cnt, pm_cnt, ht_cnt, to_cnt, 4, at<int32_t>(c, o_counts), 3));
         }
+    }
+    if (h.ext && U) {
+        // block-coded stream: copy its parts to aligned buffers, then decode every block
+        cudaStream_t xs = c->side[0];
+        const uint8_t* src = d_cont + s_gr.data_off;
+        const uint64_t pad = (8 - (2 * x_nb) % 8) % 8;
+        CUDA_TRY(cudaMemcpyAsync(at<uint8_t>(c, o_xw), src, x_nb, cudaMemcpyDeviceToDevice, xs));
+        CUDA_TRY(cudaMemcpyAsync(at<uint8_t>(c, o_xk), src + x_nb, x_nb, cudaMemcpyDeviceToDevice, xs));
+        CUDA_TRY(cudaMemcpyAsync(at<uint8_t>(c, o_xoff), src + 2 * x_nb + pad, 8 * x_nb, cudaMemcpyDeviceToDevice, xs));
+        CUDA_TRY(cudaMemsetAsync(at<uint8_t>(c, o_xpay), 0, 4 * (cdiv(x_bits, 32) + 2), xs));
+        CUDA_TRY(cudaMemcpyAsync(at<uint8_t>(c, o_xpay), src + 2 * x_nb + pad + 8 * x_nb, cdiv(x_bits, 8),
+                                 cudaMemcpyDeviceToDevice, xs));
+        Prof pr(c, "decode_blocks", 1, s_gr.data_len + 8.0 * U, xs);
+        launch_block_decode(at<uint32_t>(c, o_xpay), x_bits, U, at<uint8_t>(c, o_xw), at<uint8_t>(c, o_xk),
+                            at<unsigned long long>(c, o_xoff), at<unsigned long long>(c, o_rv), SMALL_FIELD(c, err),
+                            xs);
     }
     for (auto& j : jobs) {
         if (j.fill) {
@@ -1313,6 +1499,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     ri.blk_ids = at<unsigned long long>(c, o_blk);
     ri.nblocks = NB;
     ri.counts = at<int32_t>(c, o_counts);
+    ri.rep_val = h.ext ? at<unsigned long long>(c, o_rv) : nullptr;
     CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_rflag), 0, 4 * rtiles * 5, st));
     float* out = at<float>(c, o_out);
     Prof pr_rec(c, "recover_units", 1,
@@ -1410,6 +1597,7 @@ xnyz_status xnyz_destroy(xnyz_ctx* c) {
     if (c->h_small) cudaFreeHost(c->h_small);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->d_container) cudaFree(c->d_container);
+    if (c->d_model) cudaFree(c->d_model);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1433,6 +1621,7 @@ xnyz_status xnyz_trim(xnyz_ctx* c) {
     if (c->arena.base) cudaFree(c->arena.base);
     c->arena = Arena{};
     if (c->d_container) cudaFree(c->d_container);
+    if (c->d_model) cudaFree(c->d_model);
     c->d_container = nullptr;
     c->d_container_cap = 0;
     return XNYZ_OK;
@@ -1472,7 +1661,7 @@ xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_
     if (!xyz_is_device) {
         reserved = align_up(12 * n);
         const bool wo = sort_order != nullptr && !params->rle;
-        TRY(ensure_arena(c, make_cplan(n, wo, reserved).total + encoder_reserve(n)));
+        TRY(ensure_arena(c, make_cplan(n, wo, reserved, c->block_mode != XNYZ_BLOCKS_OFF).total + encoder_reserve(n)));
         CUDA_TRY(cudaMemcpyAsync(c->arena.base, xyz, 12 * n, cudaMemcpyHostToDevice, st));
         d_xyz = reinterpret_cast<const float*>(c->arena.base);
     }
@@ -1531,13 +1720,14 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
     cudaStream_t st = c->stream;
     CUDA_TRY(cudaEventRecord(c->ev0, st));
     CompressOut R;
-    TRY(ensure_arena(c, make_cplan(n, false, 0).total + encoder_reserve(n)));
+    TRY(ensure_arena(c, make_cplan(n, false, 0, c->block_mode != XNYZ_BLOCKS_OFF).total + encoder_reserve(n)));
     TRY(compress_run(c, xyz, n, *params, false, 0, R));
     HostPhase hpa(c, "c7_assemble_device");
     const size_t clen = R.cont.size;
     if (c->d_container_cap < clen + 64) {
         CUDA_TRY(cudaStreamSynchronize(st));
         if (c->d_container) cudaFree(c->d_container);
+    if (c->d_model) cudaFree(c->d_model);
         c->d_container = nullptr;
         const size_t want = align_up(clen + clen / 4 + 64, 1 << 20);
         CUDA_TRY(cudaMalloc(&c->d_container, want));
@@ -1668,6 +1858,97 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
     CUDA_TRY(cudaStreamSynchronize(st));
     *dev_xyz = d_out;
     *n = nout;
+    return XNYZ_OK;
+}
+
+// ---- extended container and the block-parameter predictor ---------------------------------
+xnyz_status xnyz_set_block_mode(xnyz_ctx* c, int mode) {
+    if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
+    if (mode < XNYZ_BLOCKS_OFF || mode > XNYZ_BLOCKS_GLOBAL) return fail(XNYZ_ERR_INVALID_ARG, "unknown block mode");
+    c->block_mode = mode;
+    return XNYZ_OK;
+}
+
+uint64_t xnyz_model_param_count(void) { return kParamCount; }
+
+xnyz_status xnyz_set_model(xnyz_ctx* c, const float* params, uint64_t count, float fallback_confidence) {
+    if (!c || !params) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (count != static_cast<uint64_t>(kParamCount))
+        return fail(XNYZ_ERR_INVALID_ARG, "expected " + std::to_string(kParamCount) + " parameters");
+    if (!(fallback_confidence >= 0.0f && fallback_confidence <= 1.0f))
+        return fail(XNYZ_ERR_INVALID_ARG, "fallback confidence must be in [0, 1]");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->d_model) CUDA_TRY(cudaMalloc(&c->d_model, sizeof(float) * kParamCount));
+    CUDA_TRY(cudaMemcpyAsync(c->d_model, params, sizeof(float) * kParamCount, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->fallback_conf = fallback_confidence;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_last_block_info(xnyz_ctx* c, xnyz_block_info* info) {
+    if (!c || !info) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    *info = c->last_blocks;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_stage_repos(xnyz_ctx* c, const float* dev_xyz, uint64_t n, const xnyz_params* params,
+                             uint64_t* dev_out, uint64_t cap, uint64_t* count) {
+    if (!c || !dev_xyz || !params || !count || (cap && !dev_out)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    const int mode = c->block_mode;
+    c->block_mode = XNYZ_BLOCKS_GLOBAL;
+    const uint8_t* dc = nullptr;
+    uint64_t dl = 0;
+    const xnyz_status s = xnyz_compress_device(c, dev_xyz, n, params, &dc, &dl, nullptr);
+    c->block_mode = mode;
+    if (s != XNYZ_OK) return s;
+    *count = c->last_repval_n;
+    const uint64_t m = std::min(cap, c->last_repval_n);
+    if (m) CUDA_TRY(cudaMemcpyAsync(dev_out, c->last_repval, 8 * m, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_block_features(const uint64_t* v, uint64_t n, float* feats, void* stream) {
+    if (n && (!v || !feats)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    launch_block_features(reinterpret_cast<const unsigned long long*>(v), n, feats, static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
+xnyz_status xnyz_block_search(const uint64_t* v, uint64_t n, uint8_t* w, uint8_t* k, uint32_t* cost, void* stream) {
+    if (n && (!v || !w || !k)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    launch_block_search(reinterpret_cast<const unsigned long long*>(v), n, nullptr, w, k, cost,
+                        static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
+xnyz_status xnyz_block_cost(const uint64_t* v, uint64_t n, const uint8_t* w, const uint8_t* k, uint32_t* cost,
+                            void* stream) {
+    if (n && (!v || !w || !k || !cost)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    launch_block_cost(reinterpret_cast<const unsigned long long*>(v), n, w, k, cost, static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
+xnyz_status xnyz_mlp_forward(const float* prm, const float* feats, uint64_t count, uint8_t* w, uint8_t* k, float* conf,
+                             float* logits, void* stream) {
+    if (count && (!prm || !feats || !w || !k)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    launch_mlp_forward(prm, feats, count, w, k, conf, logits, static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
+uint64_t xnyz_mlp_gather_floats(uint64_t count) { return mlp_gather_floats(count); }
+xnyz_status xnyz_mlp_train_batch(const float* prm, const float* feats, const uint8_t* w, const uint8_t* k,
+                                 const uint32_t* idx, uint64_t first, uint64_t count, float scale, float* grad,
+                                 float* loss, float* gather, void* stream) {
+    if (count && (!prm || !feats || !w || !k || !grad || !loss || !gather))
+        return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    launch_mlp_train(prm, feats, w, k, idx, first, count, scale, grad, loss, gather, static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
+    return XNYZ_OK;
+}
+xnyz_status xnyz_mlp_adam(float* prm, float* grad, float* m, float* v, float lr, int step, void* stream) {
+    if (!prm || !grad || !m || !v || step < 1) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    launch_mlp_adam(prm, grad, m, v, lr, step, static_cast<cudaStream_t>(stream));
+    CUDA_TRY(cudaGetLastError());
     return XNYZ_OK;
 }
 

@@ -69,6 +69,15 @@ std::vector<uint64_t> largest_first(uint64_t count, Size&& size) {
 
 extern "C" {
 
+xnyz_status xnyz_batch_set_block_mode(xnyz_batch* b, int mode) {
+    if (!b) return xnyz::set_last_error(XNYZ_ERR_INVALID_ARG, "null batch");
+    for (xnyz_ctx* c : b->ctx) {
+        const xnyz_status s = xnyz_set_block_mode(c, mode);
+        if (s != XNYZ_OK) return s;
+    }
+    return XNYZ_OK;
+}
+
 xnyz_status xnyz_batch_create(xnyz_batch** out, int device, int workers) {
     if (!out) return xnyz::set_last_error(XNYZ_ERR_INVALID_ARG, "null batch pointer");
     *out = nullptr;

@@ -155,6 +155,7 @@ struct RecoverArgs {
     const u64* blk_ids;
     u64 nblocks;
     const i32* counts;
+    const u64* rep_val;
     u64 units;
     u64 nout;
     RecoverParams rp;
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     for (int i = 0; i < kItems; ++i) {
         const u32 e = (u32)i * kThreads + tid;
         if (e < cnt) {
-            srep[e] = a.rep_sym[base + e];
+            srep[e] = a.rep_val ? (u8)1 : a.rep_sym[base + e];
             if (!DIRECT) {
                 squad[e] = a.quad_sym[base + e];
                 sstart[e] = a.is_start[base + e];
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     for (int i = 0; i < kItems; ++i) {
         const u32 e = e0 + i;
         if (e >= cnt) break;
-        zr += srep[e] == 0;
+        zr += !a.rep_val && srep[e] == 0;
         if (rle) csum += (u64)max(a.counts[base + e], 0);
         if (!DIRECT) {
             const bool st = sstart[e] != 0;
@@ -251,7 +252,9 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         if (e >= cnt) continue;
         const u32 sym = srep[e];
         u64 v;
-        if (sym == 0) {
+        if (a.rep_val) {
+            v = a.rep_val[base + e];
+        } else if (sym == 0) {
             if (zrun < a.npatch) {
                 v = a.rep_patch[zrun];
             } else {
@@ -395,6 +398,7 @@ void launch_recover_units(const RecoverInputs& in, uint64_t units, uint64_t nout
     a.blk_ids = in.blk_ids;
     a.nblocks = in.nblocks;
     a.counts = in.counts;
+    a.rep_val = in.rep_val;
     a.units = units;
     a.nout = nout;
     a.rp = rp;

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
         const u32 qsym = ((f >> 8) & 0xffu) + 1u;
         if (head) {
             out.rep_sym[uu] = (u8)sym;
+            if (out.rep_val) out.rep_val[uu] = val[i];
             if (!DIRECT) out.quad_sym[uu] = (u8)qsym;
             if (patch) {
                 out.patches[pp] = val[i];

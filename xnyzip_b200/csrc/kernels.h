@@ -63,6 +63,7 @@ struct UnitOutputs {
     unsigned long long* hist_quad;  // [256]
     uint32_t* first_quad;           // [256]
     unsigned long long* counters;   // [0] units, [1] patches, [2] blocks, [3] sum of patches
+    unsigned long long* rep_val;    // optional: repos / sfc delta value per unit (extended container)
 };
 
 struct LookBackState {
@@ -213,6 +214,7 @@ struct RecoverInputs {
     const unsigned long long* blk_ids;
     uint64_t nblocks;
     const int32_t* counts;         // -rle
+    const unsigned long long* rep_val;  // extended container: repos / sfc delta per unit (replaces rep_sym + patches)
 };
 void launch_block_starts(const unsigned long long* start_excl, uint64_t nblocks, uint64_t units, uint8_t* is_start,
                          uint32_t* start_block, uint32_t* err, cudaStream_t st);
@@ -221,6 +223,40 @@ void launch_recover_units(const RecoverInputs& in, uint64_t units, uint64_t nout
                           const uint8_t* hilbert_inv_tab, uint32_t* flag, unsigned long long* agg,
                           unsigned long long* inc, uint32_t* tile_counter, float* out, uint32_t* err,
                           cudaStream_t st);
+
+
+// --- block-parameter coding (extended container) and its predictor ------------------------
+constexpr int kParamBlock = 1024;     // values per block
+constexpr int kParamFeatures = 34;    // features per block (row stride of the feature array)
+constexpr int kParamInputs = 34;
+constexpr int kParamOutputsK = 32;    // Golomb-Rice k in 0..31
+constexpr int kParamOutputsW = 33;    // PFor width w in 0..32
+constexpr int kParamCount = 64 * 48 + 64 + 64 * 64 + 64 + 72 * 64 + 72;  // FP32 parameters of the MLP
+void launch_block_features(const unsigned long long* v, uint64_t n, float* feats, cudaStream_t st);
+// Exhaustive (w, k) search per block; `only` (may be null) restricts it to flagged blocks.
+void launch_block_search(const unsigned long long* v, uint64_t n, const uint8_t* only, uint8_t* w, uint8_t* k,
+                         uint32_t* cost, cudaStream_t st);
+void launch_block_cost(const unsigned long long* v, uint64_t n, const uint8_t* w, const uint8_t* k, uint32_t* cost,
+                       cudaStream_t st);
+void launch_block_offsets(const uint32_t* cost, uint64_t nblk, unsigned long long* offs, unsigned long long* total,
+                          cudaStream_t st);
+void launch_block_encode(const unsigned long long* v, uint64_t n, const uint8_t* w, const uint8_t* k,
+                         const unsigned long long* offs, uint32_t* payload, cudaStream_t st);
+void launch_block_decode(const uint32_t* payload, uint64_t payload_bits, uint64_t n, const uint8_t* w,
+                         const uint8_t* k, const unsigned long long* offs, unsigned long long* out, uint32_t* err,
+                         cudaStream_t st);
+void launch_block_fallback(const float* conf, uint64_t nblk, float thr, uint8_t* flags, unsigned long long* count,
+                           cudaStream_t st);
+// One (w = 0, k = floor(log2(mean))) pair for every block; sum: device double, zeroed.
+void launch_block_global(const unsigned long long* v, uint64_t n, double* sum, uint8_t* w, uint8_t* k,
+                         cudaStream_t st);
+void launch_mlp_forward(const float* prm, const float* feats, uint64_t count, uint8_t* w, uint8_t* k, float* conf,
+                        float* logits, cudaStream_t st);
+size_t mlp_gather_floats(uint64_t count);
+void launch_mlp_train(const float* prm, const float* feats, const uint8_t* wlab, const uint8_t* klab,
+                      const uint32_t* idx, uint64_t first, uint64_t count, float scale, float* grad, float* loss,
+                      float* gather, cudaStream_t st);
+void launch_mlp_adam(float* prm, float* grad, float* m, float* v, float lr, int step, cudaStream_t st);
 
 }  // namespace dev
 }  // namespace xnyz
