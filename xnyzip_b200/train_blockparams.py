@@ -272,7 +272,11 @@ def main(argv=None):
     from . import Context
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    ctx = Context(0, stream=torch.cuda.current_stream(dev).cuda_stream)
+    # one stream for torch's generators and the library (the legacy default stream does not
+    # order against the library's own non-blocking stream)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = Context(0, stream=stream.cuda_stream)
     F, W, K, Cst, _ = collect(ctx, _seeds(a.seeds), dev, keep_vals=False)
     Fe, We, Ke, Ce, ve = collect(ctx, _seeds(a.eval_seeds), dev)
     prm, hist, secs = train(F, W, K, a.epochs, a.batch, a.lr, dev=dev)
