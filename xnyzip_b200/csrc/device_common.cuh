@@ -169,6 +169,82 @@ struct StoreSeg {
     }
 };
 
+// Warp-cooperative look-back: called by all 32 lanes of one warp, returns the exclusive
+// prefix of `tile` to every lane and publishes its inclusive prefix.  Each step inspects 32
+// predecessors at once (lane i: tile - 1 - i - 32 * step), waits until all of them have
+// published something, then combines the aggregates up to the nearest inclusive prefix.
+// `op` need not commute: earlier tiles are combined first.
+__device__ __forceinline__ u64 shfl_down_t(u64 v, int d) { return __shfl_down_sync(kFullMask, v, d); }
+__device__ __forceinline__ Seg shfl_down_t(Seg v, int d) {
+    return Seg{__shfl_down_sync(kFullMask, v.head, d), __shfl_down_sync(kFullMask, v.sum, d)};
+}
+__device__ __forceinline__ u64 shfl_t(u64 v, int l) { return __shfl_sync(kFullMask, v, l); }
+__device__ __forceinline__ Seg shfl_t(Seg v, int l) {
+    return Seg{__shfl_sync(kFullMask, v.head, l), __shfl_sync(kFullMask, v.sum, l)};
+}
+
+template <typename T, typename Op, typename Load, typename Store>
+__device__ T warp_lookback(u32* flag, T* agg, T* inc, u32 tile, T mine, T identity, Op op, Load load, Store store,
+                           u32* err) {
+    const int lane = (int)(threadIdx.x & 31u);
+    if (tile == 0) {
+        if (lane == 0) {
+            store(&inc[0], mine);
+            __threadfence();
+            st_volatile(&flag[0], 2u);
+        }
+        __syncwarp();
+        return identity;
+    }
+    if (lane == 0) {
+        store(&agg[tile], mine);
+        __threadfence();
+        st_volatile(&flag[tile], 1u);
+    }
+    T acc = identity;
+    i64 top = (i64)tile - 1;
+    u32 spins = 0;
+    bool failed = false;
+    while (true) {
+        const i64 p = top - lane;
+        const u32 f = p >= 0 ? ld_volatile(&flag[p]) : 2u;
+        if (__any_sync(kFullMask, f == 0u)) {
+            if (++spins > kSpinLimit) {
+                failed = true;
+                break;
+            }
+            if (spins > 64) __nanosleep(100);
+            continue;
+        }
+        __threadfence();
+        T v = identity;
+        if (p >= 0) v = f == 2u ? load(&inc[p]) : load(&agg[p]);
+        const u32 m2 = __ballot_sync(kFullMask, f == 2u);
+        const int last = m2 ? __ffs(m2) - 1 : 31;
+        T r = lane <= last ? v : identity;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T o = shfl_down_t(r, d);  // lane + d: an earlier tile
+            if (lane + d < 32) r = op(o, r);
+        }
+        acc = op(shfl_t(r, 0), acc);
+        if (m2) break;
+        top -= 32;
+    }
+    if (lane == 0) {
+        if (failed) atomicOr(err, kErrTimeout);
+        store(&inc[tile], op(acc, mine));
+        __threadfence();
+        st_volatile(&flag[tile], 2u);
+    }
+    __syncwarp();
+    return acc;
+}
+
+__device__ __forceinline__ u64 warp_lookback_add(LookBack64 lb, u32 tile, u64 mine, u32* err) {
+    return warp_lookback(lb.flag, lb.agg, lb.inc, tile, mine, (u64)0, AddOp{}, LoadU64{}, StoreU64{}, err);
+}
+
 // Dynamic tile index: tiles are claimed in launch order, so a tile's predecessors have
 // all started before it waits on them.
 __device__ __forceinline__ u32 claim_tile(u32* counter, u32* smem_slot) {

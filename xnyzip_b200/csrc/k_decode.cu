@@ -50,11 +50,13 @@ __global__ void __launch_bounds__(kThreads) scan_u64_kernel(const u64* __restric
         if (e0 + i < cnt) s += sv[e0 + i];
     u64 tot;
     const u64 ex = block_exclusive<kThreads>(s, 0ull, AddOp{}, scratch, tot);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         LookBack64 l{lb.flag, lb.agg, lb.inc};
-        const u64 before = lookback_add(l, tile, tot, err);
-        sbase = before;
-        if (tile == gridDim.x - 1 && total) *total = before + tot;
+        const u64 before = warp_lookback_add(l, tile, tot, err);
+        if (threadIdx.x == 0) {
+            sbase = before;
+            if (tile == gridDim.x - 1 && total) *total = before + tot;
+        }
     }
     __syncthreads();
     u64 run = sbase + ex;
@@ -223,20 +225,28 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         eq = block_exclusive_seg(qs, scrseg, tq);
         eb = block_exclusive_seg(bs, scrseg, tb);
     }
-    if (tid == 0) {
+    // one warp per chained scan
+    const int wid = tid >> 5;
+    if (wid == 0) {
         LookBack64 l{a.flag, a.agg, a.inc};
-        base_zero = lookback_add(l, tile, tz, a.err);
-    } else if (tid == 32 && rle) {
+        const u64 r = warp_lookback_add(l, tile, tz, a.err);
+        if (tid == 0) base_zero = r;
+    } else if (wid == 1 && rle) {
         LookBack64 l{a.flag + ntiles, a.agg + 2ull * ntiles, a.inc + 2ull * ntiles};
-        base_count = lookback_add(l, tile, tc, a.err);
-    } else if (tid == 64 && !DIRECT) {
+        const u64 r = warp_lookback_add(l, tile, tc, a.err);
+        if (tid == 32) base_count = r;
+    } else if (wid == 2 && !DIRECT) {
         Seg* ag = reinterpret_cast<Seg*>(a.agg + 4ull * ntiles);
         Seg* in = reinterpret_cast<Seg*>(a.inc + 4ull * ntiles);
-        base_quad = lookback(a.flag + 2 * ntiles, ag, in, tile, tq, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
-    } else if (tid == 96 && !DIRECT) {
+        const Seg r =
+            warp_lookback(a.flag + 2 * ntiles, ag, in, tile, tq, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+        if (tid == 64) base_quad = r;
+    } else if (wid == 3 && !DIRECT) {
         Seg* ag = reinterpret_cast<Seg*>(a.agg + 6ull * ntiles);
         Seg* in = reinterpret_cast<Seg*>(a.inc + 6ull * ntiles);
-        base_blk = lookback(a.flag + 3 * ntiles, ag, in, tile, tb, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+        const Seg r =
+            warp_lookback(a.flag + 3 * ntiles, ag, in, tile, tb, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+        if (tid == 96) base_blk = r;
     }
     if (!rle && tid == 0) base_count = 0;
     __syncthreads();
@@ -278,14 +288,17 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     Seg tr{0, 0}, er{0, 0};
     if (DIRECT) ed = block_exclusive<kThreads>(dsum, 0ull, AddOp{}, scr64, td);
     else er = block_exclusive_seg(rs, scrseg, tr);
-    if (tid == 0) {
+    if (wid == 0) {
         if (DIRECT) {
             LookBack64 l{a.flag + 4 * ntiles, a.agg + 8ull * ntiles, a.inc + 8ull * ntiles};
-            base_sfc = lookback_add(l, tile, td, a.err);
+            const u64 r = warp_lookback_add(l, tile, td, a.err);
+            if (tid == 0) base_sfc = r;
         } else {
             Seg* ag = reinterpret_cast<Seg*>(a.agg + 8ull * ntiles);
             Seg* in = reinterpret_cast<Seg*>(a.inc + 8ull * ntiles);
-            base_rep = lookback(a.flag + 4 * ntiles, ag, in, tile, tr, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+            const Seg r =
+                warp_lookback(a.flag + 4 * ntiles, ag, in, tile, tr, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+            if (tid == 0) base_rep = r;
         }
     }
     __syncthreads();

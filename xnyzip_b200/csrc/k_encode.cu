@@ -131,13 +131,15 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     const u64 mine = (u64)h | ((u64)p << 21) | ((u64)b << 42);
     u64 tot;
     const u64 ex = block_exclusive<kThreads>(mine, 0ull, AddOp{}, scratch, tot);
-    if (tid == 0 || tid == 32 || tid == 64) {
+    if (tid < 96) {  // warps 0, 1, 2: one chained scan each
         const int ch = tid >> 5;
         const u64 part = (tot >> (21 * ch)) & ((1ull << 21) - 1);
         LookBack64 l{lb.flag + ch * ntiles, lb.agg + ch * ntiles, lb.inc + ch * ntiles};
-        const u64 before = lookback_add(l, tile, part, err);
-        sbase[ch] = before;
-        if (tile == ntiles - 1) out.counters[ch] = before + part;
+        const u64 before = warp_lookback_add(l, tile, part, err);
+        if ((tid & 31) == 0) {
+            sbase[ch] = before;
+            if (tile == ntiles - 1) out.counters[ch] = before + part;
+        }
     }
     __syncthreads();
 
@@ -299,11 +301,13 @@ __device__ __forceinline__ u32 stage_tile(const T* __restrict__ in, u64 n, T* s,
 
 __device__ __forceinline__ u64 tile_bit_base(LookBackState lb, u32 tile, u64 tot, u64* sbase,
                                              unsigned long long* total_bits, u32* err) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         LookBack64 l{lb.flag, lb.agg, lb.inc};
-        const u64 before = lookback_add(l, tile, tot, err);
-        *sbase = before;
-        if (tile == gridDim.x - 1) *total_bits = before + tot;
+        const u64 before = warp_lookback_add(l, tile, tot, err);
+        if (threadIdx.x == 0) {
+            *sbase = before;
+            if (tile == gridDim.x - 1) *total_bits = before + tot;
+        }
     }
     __syncthreads();
     return *sbase;

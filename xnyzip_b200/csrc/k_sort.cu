@@ -60,7 +60,7 @@ __device__ u64 digit_lookback(u64* status, u32 tile, u32 d, u64 count, u32 epoch
 }
 
 template <bool PAYLOAD>
-__global__ void __launch_bounds__(kThreads) sort_pass_kernel(const u64* __restrict__ kin, u64* __restrict__ kout,
+__global__ void __launch_bounds__(kThreads, 3) sort_pass_kernel(const u64* __restrict__ kin, u64* __restrict__ kout,
                                                              const u32* __restrict__ vin, u32* __restrict__ vout,
                                                              u64 n, int shift, const u32* __restrict__ offsets,
                                                              u64* status, u32 epoch, u32* tile_counter, u32* err) {
