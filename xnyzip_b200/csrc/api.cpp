@@ -1253,14 +1253,13 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     // ---- arena plan ----
     Plan pl;
     pl.total = reserved;
-    const size_t o_blkd = pl.add(8 * NB + 8), o_cntd = pl.add(8 * NB + 8), o_blk = pl.add(8 * NB + 8),
-                 o_cnt = pl.add(8 * NB + 8), o_start = pl.add(8 * NB + 8);
+    const size_t o_blk = pl.add(8 * NB + 8);
     const size_t o_patch = pl.add(8 * P + 8);
     const size_t o_rep = pl.add(U + 8), o_quad = pl.add(U + 8), o_isst = pl.add(U + 8), o_stb = pl.add(4 * U + 8);
     const size_t o_counts = pl.add(4 * U + 8);
     const size_t o_xw = h.ext ? pl.add(x_nb) : 0, o_xk = h.ext ? pl.add(x_nb) : 0, o_xoff = h.ext ? pl.add(8 * x_nb) : 0,
                  o_xpay = h.ext ? pl.add(4 * (cdiv(x_bits, 32) + 2)) : 0, o_rv = h.ext ? pl.add(8 * U + 8) : 0;
-    const LB lb_scan = plan_lb(pl, cdiv(std::max<uint64_t>(NB, 1), kScanTile), 3);
+    const LB lb_scan = plan_lb(pl, cdiv(std::max<uint64_t>(NB, 1), kScanTile), 4);
     struct TabOff {
         size_t root, tree, sym;
     };
@@ -1316,21 +1315,12 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         uint64_t b0, b1;
         const uint32_t* w0 = words_of(h.streams[0], b0);
         const uint32_t* w1 = words_of(h.streams[1], b1);
-        Prof pr(c, "block_streams", 6, 16.0 * NB + (w_blk + w_cnt) * NB / 8.0 + 48.0 * NB + 9.0 * NB);
-        launch_bitunpack(w0, b0, NB, w_blk, at<unsigned long long>(c, o_blkd), st);
-        launch_bitunpack(w1, b1, NB, w_cnt, at<unsigned long long>(c, o_cntd), st);
-        TRY(lb_clear(c, lb_scan, 3));
-        const LookBackState ls = lb_state(c, lb_scan);
-        auto ch = [&](int k) { return LookBackState{ls.flag + k * lb_scan.tiles, ls.agg + k * lb_scan.tiles, ls.inc + k * lb_scan.tiles}; };
-        launch_scan_u64(at<unsigned long long>(c, o_blkd), at<unsigned long long>(c, o_blk), NB, 0, ch(0),
-                        SMALL_FIELD(c, tile_counters[20]), nullptr, SMALL_FIELD(c, err), st);
-        launch_scan_u64(at<unsigned long long>(c, o_cntd), at<unsigned long long>(c, o_cnt), NB, 0, ch(1),
-                        SMALL_FIELD(c, tile_counters[21]), nullptr, SMALL_FIELD(c, err), st);
-        launch_scan_u64(at<unsigned long long>(c, o_cnt), at<unsigned long long>(c, o_start), NB, 1, ch(2),
-                        SMALL_FIELD(c, tile_counters[22]), SMALL_FIELD(c, count_total), SMALL_FIELD(c, err), st);
+        Prof pr(c, "block_streams", 1, (w_blk + w_cnt) * NB / 8.0 + 8.0 * NB + 5.0 * std::min(NB, U));
+        TRY(lb_clear(c, lb_scan, 2));
         CUDA_TRY(cudaMemsetAsync(at<uint8_t>(c, o_isst), 0, U + 8, st));
-        launch_block_starts(at<unsigned long long>(c, o_start), NB, U, at<uint8_t>(c, o_isst), at<uint32_t>(c, o_stb),
-                            SMALL_FIELD(c, err), st);
+        launch_block_streams(w0, b0, w_blk, w1, b1, w_cnt, NB, U, at<unsigned long long>(c, o_blk),
+                             at<uint8_t>(c, o_isst), at<uint32_t>(c, o_stb), lb_state(c, lb_scan),
+                             SMALL_FIELD(c, tile_counters[20]), SMALL_FIELD(c, count_total), SMALL_FIELD(c, err), st);
     }
 
     // ---- entropy-coded streams ----

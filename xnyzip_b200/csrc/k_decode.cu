@@ -73,6 +73,141 @@ __global__ void __launch_bounds__(kThreads) scan_u64_kernel(const u64* __restric
     }
 }
 
+// ------------------------------------------------------------- block streams -----------
+// The -normal/-rle block streams of block mode in one pass (block_decompressor.hpp:111-161):
+// bit-unpack the block-id deltas and block-count deltas, inclusive prefix sums of both
+// (u64, wrapping), the exclusive prefix of the counts (first unit of each block), and the
+// per-unit block-start marks of recover_from_lcp_meta (block_quantizer.hpp:167-176).
+// The count channel carries (sum of deltas, blocks, sum of counts) so that the prefix of the
+// counts and the prefix of their prefix come out of one chained scan:
+//   (A1, N1, B1) then (A2, N2, B2) = (A1 + A2, N1 + N2, B1 + B2 + N2 * A1).
+struct Tri {
+    u64 a, n, b;
+};
+struct TriOp {
+    __device__ __forceinline__ Tri operator()(Tri x, Tri y) const { return Tri{x.a + y.a, x.n + y.n, x.b + y.b + y.n * x.a}; }
+};
+struct LoadTri {
+    __device__ __forceinline__ Tri operator()(const Tri* p) const {
+        return Tri{ld_volatile(&p->a), ld_volatile(&p->n), ld_volatile(&p->b)};
+    }
+};
+struct StoreTri {
+    __device__ __forceinline__ void operator()(Tri* p, Tri v) const {
+        st_volatile(&p->a, v.a);
+        st_volatile(&p->n, v.n);
+        st_volatile(&p->b, v.b);
+    }
+};
+// found by argument-dependent lookup from warp_lookback
+__device__ __forceinline__ Tri shfl_down_t(Tri v, int d) {
+    return Tri{__shfl_down_sync(kFullMask, v.a, d), __shfl_down_sync(kFullMask, v.n, d),
+               __shfl_down_sync(kFullMask, v.b, d)};
+}
+__device__ __forceinline__ Tri shfl_t(Tri v, int l) {
+    return Tri{__shfl_sync(kFullMask, v.a, l), __shfl_sync(kFullMask, v.n, l), __shfl_sync(kFullMask, v.b, l)};
+}
+__device__ __forceinline__ Tri shfl_up_tri(Tri v, int d) {
+    return Tri{__shfl_up_sync(kFullMask, v.a, d), __shfl_up_sync(kFullMask, v.n, d), __shfl_up_sync(kFullMask, v.b, d)};
+}
+
+// Block-wide exclusive scan of Tri values (thread order).
+__device__ Tri block_exclusive_tri(Tri v, Tri* scratch, Tri& total) {
+    TriOp op;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Tri inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const Tri o = shfl_up_tri(inc, d);
+        if (lane >= d) inc = op(o, inc);
+    }
+    if (lane == 31) scratch[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        Tri x = lane < kThreads / 32 ? scratch[lane] : Tri{0, 0, 0};
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Tri o = shfl_up_tri(x, d);
+            if (lane >= d) x = op(o, x);
+        }
+        if (lane < kThreads / 32) scratch[lane] = x;
+    }
+    __syncthreads();
+    const Tri wp = w == 0 ? Tri{0, 0, 0} : scratch[w - 1];
+    Tri ex = shfl_up_tri(inc, 1);
+    if (lane == 0) ex = Tri{0, 0, 0};
+    total = scratch[kThreads / 32 - 1];
+    const Tri r = op(wp, ex);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __restrict__ wb, u64 bb, int width_b,
+                                                                 const u32* __restrict__ wc, u64 bc, int width_c,
+                                                                 u64 nb, u64 units, u64* __restrict__ blk_out,
+                                                                 u8* __restrict__ is_start, u32* __restrict__ start_block,
+                                                                 LookBackState lb, u32* tile_counter,
+                                                                 unsigned long long* count_total, u32* err) {
+    __shared__ u64 scr64[16];
+    __shared__ Tri scrtri[16];
+    __shared__ u32 slot;
+    __shared__ u64 base_b;
+    __shared__ Tri base_c;
+    const u32 tile = claim_tile(tile_counter, &slot);
+    const u32 ntiles = gridDim.x;
+    const int tid = threadIdx.x;
+    const u64 first = (u64)tile * kTile + (u64)tid * kItems;  // my blocks: first .. first + kItems - 1
+    const u64 mb = width_b >= 64 ? ~0ull : ((1ull << width_b) - 1), mc = width_c >= 64 ? ~0ull : ((1ull << width_c) - 1);
+    // the deltas are unpacked twice (the words stay in L1) rather than held in registers
+    auto delta_b = [&](u64 j) { return width_b ? (peek_lsb64(wb, bb + j * (u64)width_b) & mb) : 0ull; };
+    auto delta_c = [&](u64 j) { return width_c ? (peek_lsb64(wc, bc + j * (u64)width_c) & mc) : 0ull; };
+    u64 sb = 0, sc = 0, spc = 0;
+    u32 cnt = 0;
+    for (int i = 0; i < kItems; ++i) {
+        const u64 j = first + i;
+        if (j >= nb) break;
+        sb += delta_b(j);
+        sc += delta_c(j);
+        spc += sc;  // sum of the thread-local inclusive prefixes of the count deltas
+        ++cnt;
+    }
+    u64 tb;
+    const u64 eb = block_exclusive<kThreads>(sb, 0ull, AddOp{}, scr64, tb);
+    Tri tt;
+    const Tri ec = block_exclusive_tri(Tri{sc, (u64)cnt, spc}, scrtri, tt);
+    if (tid < 32) {
+        LookBack64 l{lb.flag, lb.agg, lb.inc};
+        const u64 r = warp_lookback_add(l, tile, tb, err);
+        if (tid == 0) base_b = r;
+    } else if (tid < 64) {
+        Tri* ag = reinterpret_cast<Tri*>(lb.agg + ntiles);
+        Tri* in = reinterpret_cast<Tri*>(lb.inc + ntiles);
+        const Tri r = warp_lookback(lb.flag + ntiles, ag, in, tile, tt, Tri{0, 0, 0}, TriOp{}, LoadTri{}, StoreTri{}, err);
+        if (tid == 32) {
+            base_c = r;
+            if (tile == ntiles - 1) *count_total = TriOp{}(r, tt).b;
+        }
+    }
+    __syncthreads();
+    u64 blk = base_b + eb;
+    const Tri pre = TriOp{}(base_c, ec);
+    u64 cntv = pre.a;   // count delta sum so far: inclusive scan gives the block counts
+    u64 start = pre.b;  // sum of the counts so far: the first unit of my first block
+    for (int i = 0; i < kItems; ++i) {
+        const u64 j = first + i;
+        if (j >= nb) break;
+        blk += delta_b(j);
+        cntv += delta_c(j);
+        blk_out[j] = blk;
+        const u64 en = start + cntv;
+        if (en > start && start < units) {  // non-empty block (the reference skips empty ones)
+            is_start[start] = 1;
+            start_block[start] = (u32)j;
+        }
+        start = en;
+    }
+}
+
 // ---------------------------------------------------------------- units --------------
 __global__ void __launch_bounds__(kThreads) block_starts_kernel(const u64* __restrict__ start_excl,
                                                                 const u64* __restrict__ blk_cnt_unused, u64 nb,
@@ -252,30 +387,26 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     __syncthreads();
 
     // ---- round 2: repos values (need the patch index) -> repos segments / SFC sums ----
-    u64 zrun = base_zero + ez;
-    u64 rv[kItems];
+    // repos value of element e; zrun: index of the next patch (advanced on symbol 0).  The
+    // values are produced here and again in the final loop (patches re-read through L1)
+    // rather than kept in a per-thread array.
+    auto rep_value = [&](u32 e, u64& zrun) -> u64 {
+        if (a.rep_val) return a.rep_val[base + e];
+        const u32 sym = srep[e];
+        if (sym) return sym - 1u;
+        const u64 z = zrun++;
+        if (z < a.npatch) return a.rep_patch[z];
+        atomicOr(a.err, kErrBadStream);
+        return 0;
+    };
+    const u64 zrun0 = base_zero + ez;
+    u64 zrun = zrun0;
     Seg rs{0, 0};
     u64 dsum = 0;
     for (int i = 0; i < kItems; ++i) {
         const u32 e = e0 + i;
-        rv[i] = 0;
         if (e >= cnt) continue;
-        const u32 sym = srep[e];
-        u64 v;
-        if (a.rep_val) {
-            v = a.rep_val[base + e];
-        } else if (sym == 0) {
-            if (zrun < a.npatch) {
-                v = a.rep_patch[zrun];
-            } else {
-                v = 0;
-                atomicOr(a.err, kErrBadStream);
-            }
-            ++zrun;
-        } else {
-            v = sym - 1u;
-        }
-        rv[i] = v;
+        const u64 v = rep_value(e, zrun);
         if (DIRECT) {
             dsum += v;
         } else {
@@ -309,12 +440,14 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     u64 opos = rle ? base_count + ec : base + e0;
     u64 sfc = base_sfc + ed;
     Seg qrun = op(base_quad, eq), brun = op(base_blk, eb), rrun = op(base_rep, er);
+    zrun = zrun0;
     for (int i = 0; i < kItems; ++i) {
         const u32 e = e0 + i;
         if (e >= cnt) break;
+        const u64 rv = rep_value(e, zrun);
         i32 cx, cy, cz;
         if (DIRECT) {
-            sfc += rv[i];
+            sfc += rv;
             const u64 m = a.rp.hilbert ? hilbert_apply(htab, sfc, a.rp.bits, 0u) : sfc;
             cx = (i32)gather3(m);
             cy = (i32)gather3(m >> 1);
@@ -323,7 +456,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
             const bool st = sstart[e] != 0;
             qrun = op(qrun, Seg{st ? 1ull : 0ull, (u64)(squad[e] ? squad[e] - 1u : 0u)});
             brun = op(brun, Seg{st ? 1ull : 0ull, st ? (u64)a.start_block[base + e] : 0ull});
-            rrun = op(rrun, Seg{(st || squad[e] != 1) ? 1ull : 0ull, rv[i]});
+            rrun = op(rrun, Seg{(st || squad[e] != 1) ? 1ull : 0ull, rv});
             const u64 quadj = qrun.sum, reposj = rrun.sum, b = brun.sum;
             if (squad[e] == 0) atomicOr(a.err, kErrBadStream);  // quad patches never occur
             const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
@@ -367,6 +500,17 @@ void launch_bitunpack(const uint32_t* words, uint64_t base_bits, uint64_t n, int
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (!blocks) return;
     bitunpack_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(words, base_bits, n, width, vals);
+}
+
+void launch_block_streams(const uint32_t* words_blk, uint64_t base_blk, int width_blk, const uint32_t* words_cnt,
+                          uint64_t base_cnt, int width_cnt, uint64_t nblocks, uint64_t units,
+                          unsigned long long* blk_ids, uint8_t* is_start, uint32_t* start_block, LookBackState lb,
+                          uint32_t* tile_counter, unsigned long long* count_total, uint32_t* err, cudaStream_t st) {
+    const unsigned tiles = (unsigned)((nblocks + kTile - 1) / kTile);
+    if (!tiles) return;
+    block_streams_kernel<<<tiles, kThreads, 0, st>>>(words_blk, base_blk, width_blk, words_cnt, base_cnt, width_cnt,
+                                                     nblocks, units, blk_ids, is_start, start_block, lb, tile_counter,
+                                                     count_total, err);
 }
 
 void launch_scan_u64(const unsigned long long* in, unsigned long long* out, uint64_t n, int exclusive,

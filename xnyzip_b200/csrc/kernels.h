@@ -216,6 +216,13 @@ struct RecoverInputs {
     const int32_t* counts;         // -rle
     const unsigned long long* rep_val;  // extended container: repos / sfc delta per unit (replaces rep_sym + patches)
 };
+// Block streams of block mode in one pass: bit-unpack (widths <= 64), inclusive prefix sums of
+// the block-id and block-count deltas, block-start marks (is_start zeroed by the caller).
+// lb: flag [2 * tiles], agg and inc [4 * tiles] u64; tiles = ceil(nblocks / 4096).
+void launch_block_streams(const uint32_t* words_blk, uint64_t base_blk, int width_blk, const uint32_t* words_cnt,
+                          uint64_t base_cnt, int width_cnt, uint64_t nblocks, uint64_t units,
+                          unsigned long long* blk_ids, uint8_t* is_start, uint32_t* start_block, LookBackState lb,
+                          uint32_t* tile_counter, unsigned long long* count_total, uint32_t* err, cudaStream_t st);
 void launch_block_starts(const unsigned long long* start_excl, uint64_t nblocks, uint64_t units, uint8_t* is_start,
                          uint32_t* start_block, uint32_t* err, cudaStream_t st);
 // flag: [5 * tiles]; agg, inc: [10 * tiles]; tiles = ceil(units / 4096)
