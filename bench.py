@@ -233,6 +233,16 @@ def run_gpu(args):
         mono_s = timed(e2e_monolithic_step, e2e_steps)
     batch.close()
 
+    # ---- learned block parameters (extended container) on the same cloud ----
+    learned = None
+    if args.learned and rank == 0:
+        learned = learned_measure(ctx, stream, d_pts, n, variants, args.steps)
+
+    # ---- the uneven batch (2048 clouds): per-cloud plain launches vs the batched path ----
+    batched = None
+    if args.batch_clouds and rank == 0 and world == 1:
+        batched = batched_measure(ctx, stream, dev, args.batch_clouds, args.workers)
+
     # ---- CPU baseline: the reference on a bounded sample (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -306,6 +316,10 @@ def run_gpu(args):
             "gpu_launches": int(launches),
             "clocks": clk,
         }
+        if learned is not None:
+            line["learned"] = learned
+        if batched is not None:
+            line["batched"] = batched
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -313,6 +327,128 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------- learned block parameters ---
+def learned_measure(ctx, stream, d_pts, n, variants, steps):
+    """Extended container on the resident cloud: pre-zstd bits/point of the repos /
+    SFC-delta stream's coding under each block mode (reference Huffman+GR container, one
+    global parameter pair, the learned predictor, exhaustive search) and the device
+    compress+decompress GB/s of the learned path against the plain path."""
+    import torch
+    import xnyzip_b200 as X
+    modes = {"reference": 0, "global": 3, "learned": 2, "exhaustive": 1}
+    out = {"bits_per_point_prezstd": {}, "block_stream_bits_per_value": {}, "fallback_fraction": {}}
+    for q, l2 in variants:
+        key = f"{QNAME[q]}_{l2}"
+        bpp, bsv = {}, {}
+        for name, m in modes.items():
+            ctx.set_block_mode(m)
+            _, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, True, True)
+            bpp[name] = round(8.0 * ln / n, 4)
+            if m:
+                bi = ctx.block_info()
+                bsv[name] = round(bi["payload_bits"] / max(1, bi["values"]), 4)
+                if name == "learned":
+                    out["fallback_fraction"][key] = round(bi["fallback_blocks"] / max(1, bi["blocks"]), 5)
+        ctx.set_block_mode(0)
+        out["bits_per_point_prezstd"][key] = bpp
+        out["block_stream_bits_per_value"][key] = bsv
+    tot = {name: sum(v[name] for v in out["bits_per_point_prezstd"].values()) for name in modes}
+    out["penalty_vs_exhaustive"] = round(tot["learned"] / tot["exhaustive"] - 1.0, 6)
+    out["gain_vs_global"] = round(1.0 - tot["learned"] / tot["global"], 6)
+    out["gain_vs_reference_container"] = round(1.0 - tot["learned"] / tot["reference"], 6)
+
+    def step(mode):
+        ctx.set_block_mode(mode)
+        for q, l2 in variants:
+            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, True, True)
+            _, nout = ctx.decompress_device(p, ln, q, l2, True)
+            if nout != n:
+                raise RuntimeError("learned round trip lost points")
+
+    rates = {}
+    for name, m in (("plain", 0), ("learned", 2)):
+        step(m)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(m)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rates[name] = 12.0 * n * len(variants) * steps / (e0.elapsed_time(e1) / 1e3) / 1e9
+    ctx.set_block_mode(0)
+    out["device_GB_s"] = {k: round(v, 3) for k, v in rates.items()}
+    out["speedup_vs_plain"] = round(rates["learned"] / rates["plain"], 4)
+    out["note"] = ("extended container: the repos / SFC-delta stream in 1024-value blocks with per-block PFor "
+                   "width and Golomb-Rice k; other streams as in the reference container; pre-zstd sizes")
+    return out
+
+
+# ------------------------------------------------------------------- the uneven batch ---
+def batched_measure(ctx, stream, dev, count, workers):
+    """Uneven batch (point counts log-uniform in [1e3, 4e6], terrain / clustered, bbox side
+    log-uniform in [10, 1e4], L2 from {0.001, 0.01, 0.1}; TO, Hilbert, -rle), resident in HBM.
+    plain: one context, per-cloud compress_device + decompress_device in order.  batched:
+    xnyz_batch_roundtrip_device with worker streams per size class chosen by
+    xnyz_batch_autotune; with the reference container and with learned block parameters.
+    Device-synchronised wall clock (the work of one step spans many streams)."""
+    import torch
+    import xnyzip_b200 as X
+    from xnyzip_b200 import synthetic_gpu as G
+    t0 = time.time()
+    clouds = G.batch_clouds(count, dev)
+    torch.cuda.synchronize(dev)
+    gen_s = time.time() - t0
+    ptrs = [c.data_ptr() for c, _ in clouds]
+    ns = [c.shape[0] for c, _ in clouds]
+    params = [(1, l2, 1, 1, 1024) for _, l2 in clouds]
+    total = float(sum(ns))
+
+    def plain_step():
+        for (c, l2), n in zip(clouds, ns):
+            p, ln = ctx.compress_device(c.data_ptr(), n, 1, l2, True, True)
+            _, nout = ctx.decompress_device(p, ln, 1, l2, True)
+            if nout != n:
+                raise RuntimeError("plain round trip lost points")
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return (time.perf_counter() - t) / reps
+
+    ctx.set_block_mode(0)
+    t_plain = timed(plain_step)
+    batch = X.Batch(0, workers)
+    out = {"clouds": count, "points": int(total), "generate_s": round(gen_s, 2)}
+    res = {"plain": t_plain}
+    for name, mode in (("batched", 0), ("batched_learned", 2)):
+        batch.set_block_mode(mode)
+        tune = batch.autotune(ptrs, ns, params)
+
+        def bstep():
+            ln, no = batch.roundtrip_device(ptrs, ns, params)
+            if list(no) != ns:
+                raise RuntimeError("batched round trip lost points")
+            return ln
+
+        res[name] = timed(bstep)
+        out[f"{name}_workers_per_class"] = tune
+        out[f"{name}_bits_per_point_prezstd"] = round(8.0 * float(bstep().sum()) / total, 4)
+    batch.close()
+    out["points_per_s"] = {k: round(total / v, 1) for k, v in res.items()}
+    out["GB_s"] = {k: round(12.0 * total / v / 1e9, 3) for k, v in res.items()}
+    out["speedup_vs_plain"] = {k: round(res["plain"] / v, 3) for k, v in res.items() if k != "plain"}
+    out["note"] = ("compress+decompress of every cloud, device-resident; size classes by point count "
+                   "(powers of four from 16K), concurrent worker streams per class from the autotuner")
+    del clouds
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------- CPU baselines ---
@@ -414,6 +550,10 @@ def main():
     ap.add_argument("--chunk", type=int, default=150_000, help="points per chunk (e2e and the reference arm)")
     ap.add_argument("--workers", type=int, default=0, help="batch worker threads (0: one per host thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-clouds", type=int, default=2048,
+                    help="clouds of the uneven batch workload (0: skip that measurement)")
+    ap.add_argument("--learned", action=argparse.BooleanOptionalAction, default=True,
+                    help="also measure the extended container with learned block parameters")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")

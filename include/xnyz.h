@@ -252,6 +252,21 @@ xnyz_status xnyz_mlp_train_batch(const float* dev_params, const float* dev_feats
 xnyz_status xnyz_mlp_adam(float* dev_params, float* dev_grad, float* dev_m, float* dev_v, float lr, int step,
                           void* stream);
 
+/* Device-resident round trip of a batch: each cloud (device points) is compressed into a
+ * device container and decompressed again on a worker; the containers never leave HBM.
+ * out_len[i] receives the container size, out_n[i] the decoded point count.  Clouds are
+ * run by size class (point counts in powers of four from 16K), largest first, each class on
+ * the number of concurrent workers xnyz_batch_autotune chose (all workers by default).  No
+ * counterpart in the reference: it is the batch form of xnyz_compress_device +
+ * xnyz_decompress_device, used to measure and verify whole batches. */
+xnyz_status xnyz_batch_roundtrip_device(xnyz_batch* batch, uint64_t count, const float* const* dev_xyz,
+                                        const uint64_t* n, const xnyz_params* params, uint64_t* out_len,
+                                        uint64_t* out_n, xnyz_status* item_status);
+/* Times the round trip on a sample of each size class with 1, 2, 4, ... workers and keeps the
+ * fastest per class (class_workers, may be NULL, receives the 6 choices). */
+xnyz_status xnyz_batch_autotune(xnyz_batch* batch, uint64_t count, const float* const* dev_xyz, const uint64_t* n,
+                                const xnyz_params* params, int* class_workers);
+
 /* ---- allocation-free entry point ---------------------------------------------------------- */
 
 /* No counterpart in the reference.  The stable LSD radix sort of xnyz_stage_sort for callers

@@ -273,13 +273,14 @@ def test_learned_mode_roundtrip_and_fallback(xnyz, ctx):
     x = S.terrain(200_000, 31, extent=2000.0, amplitude=10.0, wavelength=700.0)
     ref = ctx.decompress(ctx.compress(x, 1, 0.01, 1, 1), 1, 0.01, 1)
     p = B.init_params(4)
-    for thr in (0.0, 1.0):  # no fallback / every block falls back to the exhaustive search
-        ctx.set_model(p, thr)
-        ctx.set_block_mode(2)
-        try:
-            fr = ctx.compress(x, 1, 0.01, 1, 1)
-            info = ctx.block_info()
-        finally:
-            ctx.set_block_mode(0)
-        assert ctx.decompress(fr, 1, 0.01, 1).tobytes() == ref.tobytes()
-        assert info["fallback_blocks"] == (0 if thr == 0.0 else info["blocks"])
+    own = xnyz.Context(0)  # an untrained model on a context of its own
+    try:
+        for thr in (0.0, 1.0):  # no fallback / every block falls back to the exhaustive search
+            own.set_model(p, thr)
+            own.set_block_mode(2)
+            fr = own.compress(x, 1, 0.01, 1, 1)
+            info = own.block_info()
+            assert ctx.decompress(fr, 1, 0.01, 1).tobytes() == ref.tobytes()
+            assert info["fallback_blocks"] == (0 if thr == 0.0 else info["blocks"])
+    finally:
+        own.close()

@@ -53,3 +53,32 @@ def test_batch_reports_failing_item(xnyz):
         assert st[2] == 1 and st[[0, 1, 3, 4, 5, 6, 7]].sum() == 0
     finally:
         b.close()
+
+
+def test_batch_roundtrip_device_and_autotune(xnyz, ctx):
+    """Device round trip of an uneven batch on worker streams, by size class, with the
+    autotuned worker counts: every container has the size of a lone compress_device call and
+    decodes to all its points; also with learned block parameters."""
+    import torch
+    from xnyzip_b200 import synthetic as S
+    sizes = [700, 5_000, 20_000, 70_000, 300_000, 1_100_000]
+    clouds = [torch.from_numpy(S.terrain(n, 40 + i, extent=200.0 + 50 * i, amplitude=2.0, wavelength=90.0)).cuda()
+              for i, n in enumerate(sizes)]
+    params = [(1, (0.01, 0.05, 0.1)[i % 3], i % 2, 1, 1024) for i in range(len(sizes))]
+    ptrs = [c.data_ptr() for c in clouds]
+    b = xnyz.Batch(0, 4)
+    one = xnyz.Context(0)  # a fresh context: the shipped predictor, like the batch's workers
+    try:
+        for mode in (0, 2):
+            one.set_block_mode(mode)
+            b.set_block_mode(mode)
+            want = [one.compress_device(c.data_ptr(), n, q, l2, h, r, dt)[1]
+                    for c, n, (q, l2, h, r, dt) in zip(clouds, sizes, params)]
+            tune = b.autotune(ptrs, sizes, params)
+            assert len(tune) == 6 and all(0 <= w <= 4 for w in tune)
+            ln, no = b.roundtrip_device(ptrs, sizes, params)
+            assert ln.tolist() == want
+            assert no.tolist() == sizes
+    finally:
+        one.close()
+        b.close()

@@ -216,6 +216,34 @@ class Batch:
         N.check(s)
         return frames
 
+    def set_block_mode(self, mode: int):
+        N.check(N.batch_set_block_mode(self.handle, int(mode)))
+
+    @staticmethod
+    def _device_args(ptrs, ns, params):
+        k = len(ptrs)
+        xs = (C.c_void_p * k)(*[C.c_void_p(p) for p in ptrs])
+        nn = np.ascontiguousarray(ns, dtype=np.uint64)
+        prm = (Params * k)(*[Params(int(q), float(l2), int(bool(h)), int(bool(r)), int(dt)) for q, l2, h, r, dt in params])
+        return k, xs, nn, prm
+
+    def roundtrip_device(self, ptrs, ns, params):
+        """Device points (pointers, counts, (quantizer, l2, hilbert, rle, direct_threshold)) ->
+        (container bytes, decoded point counts) of each cloud; containers stay in HBM."""
+        k, xs, nn, prm = self._device_args(ptrs, ns, params)
+        ln = np.zeros(k, np.uint64)
+        no = np.zeros(k, np.uint64)
+        N.check(N.batch_roundtrip_device(self.handle, k, xs, nn.ctypes.data_as(C.c_void_p), prm,
+                                         ln.ctypes.data_as(C.c_void_p), no.ctypes.data_as(C.c_void_p), None))
+        return ln, no
+
+    def autotune(self, ptrs, ns, params):
+        """Workers per size class, chosen by timing the device round trip on samples."""
+        k, xs, nn, prm = self._device_args(ptrs, ns, params)
+        w = np.zeros(6, np.int32)
+        N.check(N.batch_autotune(self.handle, k, xs, nn.ctypes.data_as(C.c_void_p), prm, w.ctypes.data_as(C.c_void_p)))
+        return w.tolist()
+
     def decompress(self, frames, params, outs, is_zstd: bool = True):
         """frames: sequence of bytes; params: (quantizer, l2, rle) per frame; outs: C-contiguous
         float32 arrays (e.g. views of pinned memory) receiving the points.  Returns the point

@@ -317,6 +317,118 @@ __device__ __forceinline__ u64 entry_offset(const Src& s, u32 i, u64 Bsub, int k
     return i;
 }
 
+// Golomb-Rice transition table of one subsequence [B, Bend) by lockstep simulation.  The
+// codeword-start map f(s) = z(s) + 1 + k (z(s): first zero bit at or after s) is monotone, so
+// the chains of entries 0..k keep their order, merge when they land on one position, and at
+// step n all lie within codeword n of entry 0's chain.  While that codeword is shorter than
+// 64 bits (k <= 30 and a unary part below 64 - k - 1 bits), the active chains are a 64-bit
+// position mask over a shared 128-bit zero window, and their entries a boundary mask over
+// 0..k.  Entry k + 1 (a unary run crossing B) is entry 0's chain after its first codeword.
+// Called by every thread of the warp (valid: this thread owns a subsequence); the loops are
+// warp-uniform (__any_sync) so that lanes with different chain counts stay converged.
+// Returns false (table incomplete) when a codeword is too long for the masks or the stream
+// ends within reach; the caller then runs the generic loop.
+__device__ bool gr_lockstep_table(const Src& src, u64 B, u64 Bend, int k, u32* tab, int t, bool valid) {
+    const u32 span = valid ? (u32)(Bend - B) : 0u;
+    const bool full = span == (u32)S;
+    // near the end of the stream codewords may run past it (the generic decoder gives those
+    // a length that ends the chain): left to the generic loop
+    bool ok = valid && B + span + 192 <= src.total_bits;
+    const int ne = min(k + 1, (int)span);  // entries with a codeword start inside
+    if (ok)
+        for (int e = ne; e <= k; ++e) tab[e * T + t] = kOOD;  // (only in a short last subsequence)
+    u64 act = ok ? (ne >= 64 ? ~0ull : ((1ull << ne) - 1ull)) : 0ull;  // group positions - base
+    u64 gb = act;     // first entry of every group
+    u64 alive = act;  // entries not yet recorded
+    u32 base = 0, n = 0, exit0 = kOOD, count0 = 0;
+    while (__any_sync(kFullMask, act != 0ull)) {
+        u64 z0 = 0, z1 = 0;
+        if (act) {
+            z0 = ~src.lsb64(B + base);
+            z1 = ~src.lsb64(B + base + 64);
+            ++n;
+        }
+        // successors, in order; groups landing on the previous group's position merge
+        u64 a = act, g = gb, nact = 0, ngb = gb;
+        u32 first_s = 0, prev_s = 0xffffffffu;
+        bool any = false;
+        while (__any_sync(kFullMask, a != 0ull)) {
+            if (!a) continue;
+            const int j = __ffsll((long long)a) - 1;
+            a &= a - 1;
+            const int e0 = __ffsll((long long)g) - 1;
+            g &= g - 1;
+            u32 zp = 0;
+            if (z0 >> j) {
+                zp = base + (u32)j + (u32)(__ffsll((long long)(z0 >> j)) - 1);
+            } else if (z1) {
+                zp = base + 64u + (u32)(__ffsll((long long)z1) - 1);
+            } else {  // a unary run longer than the window
+                ok = false;
+                a = 0;
+                continue;
+            }
+            const u32 sp = zp + 1u + (u32)k;
+            if (sp == prev_s) {
+                ngb &= ~(1ull << e0);
+                continue;
+            }
+            if (!any) {
+                first_s = sp;
+                any = true;
+            }
+            if (sp - first_s >= 64u) {  // the chains span more than 64 bits
+                ok = false;
+                a = 0;
+                continue;
+            }
+            nact |= 1ull << (sp - first_s);
+            prev_s = sp;
+        }
+        if (!ok) {
+            act = 0;
+            continue;
+        }
+        if (!act) continue;
+        act = nact;
+        gb = ngb;
+        base = first_s;
+        // groups at or past the end leave: they are the top groups, entries from their first
+        // entry up to the next group's first entry (or the last alive entry)
+        const u32 lo = span > base ? span - base : 0u;  // first leaving bit
+        const u64 leave = lo >= 64 ? 0ull : (act >> lo) << lo;
+        if (leave) {
+            u64 a2 = act, g2 = gb;
+            while (a2) {
+                const int j = __ffsll((long long)a2) - 1;
+                a2 &= a2 - 1;
+                const int e0 = __ffsll((long long)g2) - 1;
+                g2 &= g2 - 1;
+                if (!((leave >> j) & 1ull)) continue;
+                const int e1 = g2 ? __ffsll((long long)g2) - 1 : 64;  // next group's first entry
+                const u32 P = base + (u32)j;
+                const u32 ox = full ? entry_index<kCodeGolombRice>((u64)P - S, k + 2, k) : kOOD;
+                const u64 below1 = e1 >= 64 ? ~0ull : ((1ull << e1) - 1ull), below0 = (1ull << e0) - 1ull;
+                u64 m = alive & below1 & ~below0;
+                while (m) {
+                    const int e = __ffsll((long long)m) - 1;
+                    m &= m - 1;
+                    tab[e * T + t] = ox | (n << 8);
+                    if (e == 0) {
+                        exit0 = ox;
+                        count0 = n;
+                    }
+                }
+                alive &= ~below1 | below0;
+            }
+            act &= ~leave;
+            gb &= alive;
+        }
+    }
+    if (ok) tab[(k + 1) * T + t] = exit0 | ((count0 - 1u) << 8);
+    return ok;
+}
+
 struct Args {
     const u32* words;
     u32 base;
@@ -407,7 +519,9 @@ __global__ void __launch_bounds__(T) decode_stream_kernel(Args a) {
     const u64 Bend = min(B + S, a.total_bits);
 
     // ---- 1. transition table of my subsequence ----
-    if ((u32)t < nvalid) {
+    bool done1 = false;
+    if (KIND == kCodeGolombRice && gk <= 30) done1 = gr_lockstep_table(src, B, Bend, gk, tab, t, (u32)t < nvalid);
+    if ((u32)t < nvalid && !done1) {
         u32 rx[R] = {}, rc[R] = {};
         int nroots = 0;
         auto bmw = [&](int r, int w) -> u32& { return bm[(r * WINW + w) * T + t]; };

@@ -39,50 +39,7 @@ def _torch():
     return torch
 
 
-# ------------------------------------------------------------------ GPU generators ------
-def gen_uniform(n, seed, dev):
-    torch = _torch()
-    g = torch.Generator(device=dev).manual_seed(seed)
-    return torch.rand((n, 3), generator=g, device=dev, dtype=torch.float64).mul_(1000.0).float()
-
-
-def gen_terrain(n, seed, dev, extent=10000.0, amplitude=50.0, wavelength=5000.0, dup=0.05):
-    torch = _torch()
-    g = torch.Generator(device=dev).manual_seed(seed)
-    nd = int(round(n * dup))
-    nb = n - nd
-    ang = torch.rand(8, generator=g, device=dev, dtype=torch.float64) * 2 * math.pi
-    ph = torch.rand(8, generator=g, device=dev, dtype=torch.float64) * 2 * math.pi
-    xy = torch.rand((nb, 2), generator=g, device=dev, dtype=torch.float64) * extent
-    z = torch.randn(nb, generator=g, device=dev, dtype=torch.float64) * 0.1
-    for k in range(8):
-        d = torch.stack([torch.cos(ang[k]), torch.sin(ang[k])])
-        z += amplitude * 0.5 ** k * torch.sin(2 * math.pi * (xy @ d) / (wavelength * 0.5 ** k) + ph[k])
-    base = torch.cat([xy, z[:, None]], 1).float()
-    if nd:
-        src = torch.randint(0, nb, (nd,), generator=g, device=dev)
-        cp = base[src].clone()
-        cp[:, 2] = (cp[:, 2].double() - torch.rand(nd, generator=g, device=dev, dtype=torch.float64) * 2).float()
-        base = torch.cat([base, cp], 0)
-    return base.contiguous()
-
-
-def gen_spheres(n, seed, dev, k=20000, extent=1e5, r_median=20.0, r_sigma=0.4, jitter=0.2):
-    torch = _torch()
-    g = torch.Generator(device=dev).manual_seed(seed)
-    c = torch.rand((k, 3), generator=g, device=dev, dtype=torch.float64) * extent
-    r = torch.exp(math.log(r_median) + r_sigma * torch.randn(k, generator=g, device=dev, dtype=torch.float64))
-    w = r * r
-    quota = w / w.sum() * n
-    cnt = torch.floor(quota).long()
-    rest = n - int(cnt.sum())
-    if rest:
-        cnt[torch.argsort(-(quota - cnt), stable=True)[:rest]] += 1
-    owner = torch.repeat_interleave(torch.arange(k, device=dev), cnt)
-    u = torch.randn((n, 3), generator=g, device=dev, dtype=torch.float64)
-    u /= u.norm(dim=1, keepdim=True)
-    rr = r[owner] + jitter * torch.randn(n, generator=g, device=dev, dtype=torch.float64)
-    return (c[owner] + rr[:, None] * u).float().contiguous()
+from .synthetic_gpu import gen_spheres, gen_terrain, gen_uniform  # noqa: E402
 
 
 def workloads(seed):
