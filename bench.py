@@ -16,6 +16,17 @@ copies), Hilbert curve, -rle container, both quantizers (to, cube) x L2 bounds
           cuts the cloud into --chunk-point pieces, one frame each, exactly the workload the
           reference arm runs; `monolithic` is one frame per variant for the whole cloud.
   bits/point per variant from the zstd frame.
+  roofline: the dominant stage of one extra (untimed) step profiled with per-stage CUDA
+          events and side-stream work serialised (xnyz_profile mode 2).
+  learned : the extended container on the same cloud (block parameters of the repos /
+          SFC-delta stream: reference coding, one global pair, learned, exhaustive): pre-zstd
+          bits/point, penalty against exhaustive search, device GB/s against plain.
+  batched : the uneven batch (2048 clouds, ~1e9 points, log-uniform sizes), per-cloud plain
+          launches on one context against xnyz_batch_roundtrip_device (autotuned worker
+          streams per size class), with the reference container and with learned parameters.
+
+--workload spheres: the clustered-surface cloud instead (175M points on 200,000 spheres, TO,
+L2 0.5, Morton, -normal and -rle).
 
 --gpus N: one process per GPU (torchrun); the path does not shard, every rank runs its
 own replica on its own cloud (seed 1 + rank): weak scaling, max time over ranks.
@@ -39,7 +50,19 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-VARIANTS = [(1, 0.001), (1, 0.01), (1, 0.1), (0, 0.001), (0, 0.01), (0, 0.1)]  # (quantizer, l2)
+# workloads: (generator, default points, [(quantizer, l2, hilbert, rle)])
+WORKLOADS = {
+    # terrain-LiDAR plain method: both quantizers x L2 {0.001, 0.01, 0.1}, Hilbert, -rle
+    "terrain": ("terrain", 64_000_000, [(1, 0.001, 1, 1), (1, 0.01, 1, 1), (1, 0.1, 1, 1),
+                                        (0, 0.001, 1, 1), (0, 0.01, 1, 1), (0, 0.1, 1, 1)]),
+    # clustered surfaces: 200,000 spheres, TO, L2 0.5, Morton, -normal and -rle
+    "spheres": ("spheres", 175_000_000, [(1, 0.5, 0, 0), (1, 0.5, 0, 1)]),
+}
+
+
+def vname(v):
+    q, l2, hil, rle = v
+    return f"{QNAME[q]}_{l2}" + ("" if (hil, rle) == (1, 1) else f"_{'h' if hil else 'z'}_{'rle' if rle else 'normal'}")
 QNAME = {0: "cube", 1: "to"}
 METRIC = "compress+decompress GB/s (12 B/point input) at fixed L2 bound"
 
@@ -103,8 +126,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_cloud(n: int, seed: int):
+def make_cloud(workload: str, n: int, seed: int):
     from xnyzip_b200 import synthetic as S
+    if WORKLOADS[workload][0] == "spheres":
+        return S.spheres(n, 200_000, seed + 1)
     return S.terrain(n, seed)
 
 
@@ -129,14 +154,14 @@ def run_gpu(args):
     torch.cuda.set_stream(stream)
     ctx = X.Context(local, stream=stream.cuda_stream)
 
-    n = args.points
+    n = args.points or WORKLOADS[args.workload][1]
     t0 = time.time()
-    host = make_cloud(n, 1 + rank)
+    host = make_cloud(args.workload, n, 1 + rank)
     log(f"[rank {rank}] generated {n} points in {time.time() - t0:.1f}s")
     pinned = torch.from_numpy(host).pin_memory()
     d_pts = pinned.to(dev, non_blocking=False)
     torch.cuda.synchronize(dev)
-    variants = VARIANTS[: args.variants]
+    variants = WORKLOADS[args.workload][2][: args.variants]
 
     def barrier():
         if world > 1:
@@ -152,10 +177,10 @@ def run_gpu(args):
     # ---- device-resident step ----
     def device_step():
         containers = []
-        for q, l2 in variants:
-            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, True, True)
+        for q, l2, hil, rle in variants:
+            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
             containers.append(ln)
-            _, nout = ctx.decompress_device(p, ln, q, l2, True)
+            _, nout = ctx.decompress_device(p, ln, q, l2, rle)
             if nout != n:
                 raise RuntimeError(f"decoded {nout} points, expected {n}")
         return containers
@@ -166,7 +191,6 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     clocks = ClockSampler(local)
     clocks.start()
-    ctx.profile(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -174,13 +198,19 @@ def run_gpu(args):
         clens = device_step()
     ev1.record(stream)
     torch.cuda.synchronize(dev)
-    prof_all = ctx.profile_read()
-    ctx.profile(False)
-    prof = {k: v for k, v in prof_all.items() if not k.startswith("host:")}
-    host_phases = {k[5:]: round(v["ms"] / args.steps, 3) for k, v in prof_all.items() if k.startswith("host:")}
     clk = clocks.stop()
     dev_ms = ev0.elapsed_time(ev1)
     dev_ms = max_over_ranks(dev_ms)
+    barrier()
+    # one more step with per-stage CUDA events, the side streams' work issued on the context's
+    # stream (xnyz_profile mode 2), so that each stage's time is its own: the roofline
+    ctx.profile(2)
+    device_step()
+    prof_all = ctx.profile_read()
+    ctx.profile(False)
+    prof = {k: v for k, v in prof_all.items() if not k.startswith("host:")}
+    host_phases = {k[5:]: round(v["ms"], 3) for k, v in prof_all.items() if k.startswith("host:")}
+    torch.cuda.synchronize(dev)
     barrier()
 
     # ---- end-to-end through the host-buffer C ABI: batches of independent calls ----
@@ -192,12 +222,12 @@ def run_gpu(args):
     outs = [torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy() for _ in variants]
     bounds = [(a, min(n, a + args.chunk)) for a in range(0, n, args.chunk)]
     c_clouds = [host_np[a:b] for _ in variants for (a, b) in bounds]
-    c_params = [(q, l2, True, True) for (q, l2) in variants for _ in bounds]
-    c_dparams = [(q, l2, True) for (q, l2) in variants for _ in bounds]
+    c_params = [(q, l2, hil, rle) for (q, l2, hil, rle) in variants for _ in bounds]
+    c_dparams = [(q, l2, rle) for (q, l2, hil, rle) in variants for _ in bounds]
     c_outs = [outs[vi][a:b] for vi in range(len(variants)) for (a, b) in bounds]
     m_clouds = [host_np for _ in variants]
-    m_params = [(q, l2, True, True) for (q, l2) in variants]
-    m_dparams = [(q, l2, True) for (q, l2) in variants]
+    m_params = [(q, l2, hil, rle) for (q, l2, hil, rle) in variants]
+    m_dparams = [(q, l2, rle) for (q, l2, hil, rle) in variants]
     frame_bytes = {}
     chunk_bytes = {}
 
@@ -206,16 +236,16 @@ def run_gpu(args):
         ns = batch.decompress(frames, c_dparams, c_outs)
         if ns != [b - a for _ in variants for (a, b) in bounds]:
             raise RuntimeError("e2e (chunked) decode size mismatch")
-        for vi, (q, l2) in enumerate(variants):
-            chunk_bytes[(q, l2)] = sum(len(f) for f in frames[vi * len(bounds):(vi + 1) * len(bounds)])
+        for vi, v in enumerate(variants):
+            chunk_bytes[v] = sum(len(f) for f in frames[vi * len(bounds):(vi + 1) * len(bounds)])
 
     def e2e_monolithic_step():
         frames = batch.compress(m_clouds, m_params, as_bytes=False)
         ns = batch.decompress(frames, m_dparams, outs)
         if ns != [n] * len(variants):
             raise RuntimeError("e2e decode size mismatch")
-        for (q, l2), f in zip(variants, frames):
-            frame_bytes[(q, l2)] = len(f)
+        for v, f in zip(variants, frames):
+            frame_bytes[v] = len(f)
 
     def timed(fn, steps):
         fn()  # warm-up: worker arenas and pinned staging reach their sizes
@@ -261,8 +291,8 @@ def run_gpu(args):
         achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
         stage_bytes = sum(v["bytes"] for v in prof.values())
         stage_ms = sum(v["ms"] for v in prof.values())
-        launches = sum(v["launches"] for v in prof.values())
-        bpp = {f"{QNAME[q]}_{l2}": round(8.0 * frame_bytes[(q, l2)] / n, 4) for q, l2 in variants if (q, l2) in frame_bytes}
+        launches = sum(v["launches"] for v in prof.values()) * args.steps  # prof covers one step
+        bpp = {vname(v): round(8.0 * frame_bytes[v] / n, 4) for v in variants if v in frame_bytes}
         line = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -275,16 +305,17 @@ def run_gpu(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32 in, int32/u64 lattice and key arithmetic",
-            "data": "synthetic terrain-LiDAR stand-in (seeded, 64M points), generated on the host",
+            "data": (f"synthetic {'terrain-LiDAR' if args.workload == 'terrain' else 'clustered-surface'} "
+                     f"stand-in (seeded, {n} points), generated on the host"),
             "config": {
-                "workload": f"terrain {n} points, Hilbert, -rle, quantizers to/cube x L2 {{0.001,0.01,0.1}}; "
-                            f"one step = compress+decompress of all {len(variants)} variants",
+                "workload": (f"terrain {n} points, Hilbert, -rle, quantizers to/cube x L2 {{0.001,0.01,0.1}}"
+                             if args.workload == "terrain" else
+                             f"spheres {n} points on 200,000 spheres, TO, L2 0.5, Morton, -normal and -rle")
+                            + f"; one step = compress+decompress of all {len(variants)} variants",
                 "points": n,
-                "variants": [f"{QNAME[q]}:{l2}" for q, l2 in variants],
-                "curve": "hilbert",
-                "container": "rle",
+                "variants": [vname(v) for v in variants],
                 "direct_threshold": 1024,
-                "l2_flush": "inputs (768 MB per cloud) exceed the 126 MB L2",
+                "l2_flush": f"inputs ({12 * n / 1e6:.0f} MB per cloud) exceed the 126 MB L2",
                 "value_path": "device-resident points and pre-zstd container",
                 "e2e_path": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
                             "xnyz_batch_compress / xnyz_batch_decompress",
@@ -297,8 +328,7 @@ def run_gpu(args):
                      "workload": f"{len(bounds)} chunks of {args.chunk} points x {len(variants)} variants "
                                  f"(the reference arm's per-chunk mode), one zstd frame per chunk, "
                                  f"xnyz_batch_* with {batch.workers} worker threads",
-                     "bits_per_point": {f"{QNAME[q]}_{l2}": round(8.0 * chunk_bytes[(q, l2)] / n, 4)
-                                        for q, l2 in variants},
+                     "bits_per_point": {vname(v): round(8.0 * chunk_bytes[v] / n, 4) for v in variants},
                      "monolithic": {"value": round(mono, 4), "unit": "GB/s", "s_per_step": round(mono_s / e2e_steps, 4),
                                     "workload": "the whole cloud, one zstd frame per variant, "
                                                 f"{len(variants)} variants in one batch"}}
@@ -309,9 +339,10 @@ def run_gpu(args):
                          "bytes_per_launch": per_launch_bytes, "ms_per_launch": round(per_launch_ms, 4),
                          "pipeline_achieved": round(stage_bytes / (stage_ms / 1e3) / 1e9, 1),
                          "pipeline_frac": round(stage_bytes / (stage_ms / 1e3) / 1e9 / peak, 4)},
-            "stages": {k: {"ms_per_step": round(v["ms"] / args.steps, 4), "launches": v["launches"] // args.steps,
+            "stages": {k: {"ms_per_step": round(v["ms"], 4), "launches": v["launches"],
                            "GB_s": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None}
                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
+            "stages_note": "one extra step (not timed) with per-stage CUDA events, side-stream work serialised",
             "host_phases_ms_per_step": host_phases,
             "gpu_launches": int(launches),
             "clocks": clk,
@@ -339,12 +370,13 @@ def learned_measure(ctx, stream, d_pts, n, variants, steps):
     import xnyzip_b200 as X
     modes = {"reference": 0, "global": 3, "learned": 2, "exhaustive": 1}
     out = {"bits_per_point_prezstd": {}, "block_stream_bits_per_value": {}, "fallback_fraction": {}}
-    for q, l2 in variants:
-        key = f"{QNAME[q]}_{l2}"
+    for v in variants:
+        q, l2, hil, rle = v
+        key = vname(v)
         bpp, bsv = {}, {}
         for name, m in modes.items():
             ctx.set_block_mode(m)
-            _, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, True, True)
+            _, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
             bpp[name] = round(8.0 * ln / n, 4)
             if m:
                 bi = ctx.block_info()
@@ -361,9 +393,9 @@ def learned_measure(ctx, stream, d_pts, n, variants, steps):
 
     def step(mode):
         ctx.set_block_mode(mode)
-        for q, l2 in variants:
-            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, True, True)
-            _, nout = ctx.decompress_device(p, ln, q, l2, True)
+        for q, l2, hil, rle in variants:
+            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
+            _, nout = ctx.decompress_device(p, ln, q, l2, rle)
             if nout != n:
                 raise RuntimeError("learned round trip lost points")
 
@@ -468,14 +500,14 @@ def cpu_baseline(host, variants, sample_points, threads=1):
     if kind == "reference":
         lib.quiet(True)
     try:
-        for q, l2 in variants:
+        for q, l2, hil, rle in variants:
             if kind == "reference":
-                tc, td, _, _ = lib.roundtrip_timed(x, QNAME[q], l2, 1, 1)
+                tc, td, _, _ = lib.roundtrip_timed(x, QNAME[q], l2, hil, rle)
             else:
                 t0 = time.perf_counter()
-                fr = lib.compress(x, QNAME[q], l2, 1, 1)
+                fr = lib.compress(x, QNAME[q], l2, hil, rle)
                 t1 = time.perf_counter()
-                lib.decompress(fr, QNAME[q], l2, 1)
+                lib.decompress(fr, QNAME[q], l2, rle)
                 tc, td = t1 - t0, time.perf_counter() - t1
             tot_t += tc + td
     finally:
@@ -497,17 +529,17 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     chunk = args.chunk
     n_total = chunk * threads
-    host = make_cloud(n_total, 1)
-    variants = VARIANTS[: args.variants]
+    host = make_cloud(args.workload, n_total, 1)
+    variants = WORKLOADS[args.workload][2][: args.variants]
     if kind == "reference":
         lib.quiet(True)
 
     def step():
         def work(t):
             x = host[t * chunk:(t + 1) * chunk]
-            for q, l2 in variants:
-                fr = lib.compress(x, QNAME[q], l2, 1, 1)
-                lib.decompress(fr, QNAME[q], l2, 1)
+            for q, l2, hil, rle in variants:
+                fr = lib.compress(x, QNAME[q], l2, hil, rle)
+                lib.decompress(fr, QNAME[q], l2, rle)
         ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
         for th in ths:
             th.start()
@@ -525,13 +557,13 @@ def run_reference(args):
         if kind == "reference":
             lib.quiet(False)
     value = 12.0 * n_total * len(variants) * args.steps / dt / 1e9
-    sample = (f"{threads} threads x {chunk}-point chunks of the terrain cloud (the reference's per-chunk mode), "
+    sample = (f"{threads} threads x {chunk}-point chunks of the {args.workload} cloud (the reference's per-chunk mode), "
               f"all {len(variants)} variants per step")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"terrain, Hilbert, -rle, {len(variants)} variants; host CPU reference", "points": n_total},
+        "config": {"workload": f"{args.workload}, {len(variants)} variants; host CPU reference", "points": n_total},
         "cpu_baseline": {"value": round(value, 5), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 5), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -543,7 +575,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="xnyz", choices=["xnyz", "reference"])
-    ap.add_argument("--points", type=int, default=64_000_000)
+    ap.add_argument("--workload", default="terrain", choices=sorted(WORKLOADS))
+    ap.add_argument("--points", type=int, default=0, help="points of the cloud (0: the workload's size)")
     ap.add_argument("--variants", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-points", type=int, default=1_000_000)

@@ -44,7 +44,7 @@ def _bitlen(x: np.ndarray) -> np.ndarray:
 
 def esc_len(e: np.ndarray, k: int) -> np.ndarray:
     q = np.asarray(e, dtype=np.uint64) >> np.uint64(k)
-    return np.where(q < 32, q.astype(np.int64) + 1 + k, 96)
+    return np.where(q < 32, q.astype(np.int64) + 1 + k, 97 + k)
 
 
 def block_cost(v: np.ndarray, w: int, k: int) -> int:
@@ -113,7 +113,9 @@ class _Bits:
 
 
 def encode(vals: np.ndarray, W: np.ndarray, K: np.ndarray):
-    """(offsets, payload bytes, payload bits) of the block-coded stream."""
+    """(offsets, payload bytes, payload bits) of the block-coded stream.  Per block: w-bit
+    slots, then the unary parts of the escapes (min(q, 32) ones and a zero each), their k-bit
+    remainders, and the 64-bit values of the capped escapes (q >= 32)."""
     vals = [int(x) for x in np.asarray(vals, dtype=np.uint64)]
     nb = len(W)
     bits = _Bits()
@@ -127,19 +129,18 @@ def encode(vals: np.ndarray, W: np.ndarray, K: np.ndarray):
         for i, v in enumerate(x):
             bits.put(pos + i * w, thr if v >= thr else v, w)
         pos += len(x) * w
-        for v in x:
-            if v < thr:
-                continue
-            e = v - thr
-            q = e >> k
-            if q < 32:
-                bits.put(pos, (1 << q) - 1, q + 1)
-                bits.put(pos + q + 1, e, k)
-                pos += q + 1 + k
-            else:
-                bits.put(pos, 0xFFFFFFFF, 32)
-                bits.put(pos + 32, e, 64)
-                pos += 96
+        esc = [v - thr for v in x if v >= thr]
+        for e in esc:  # U
+            q = min(e >> k, 32)
+            bits.put(pos, (1 << q) - 1, q + 1)
+            pos += q + 1
+        for e in esc:  # R
+            bits.put(pos, e, k)
+            pos += k
+        for e in esc:  # X
+            if e >> k >= 32:
+                bits.put(pos, e, 64)
+                pos += 64
     return offs, bits.to_bytes(pos), pos
 
 
@@ -161,18 +162,29 @@ def decode(payload: bytes, nbits: int, n: int, W, K, offs) -> np.ndarray:
         base = int(offs[b])
         slots = [get(base + i * w, w) if w else 0 for i in range(cnt)]
         pos = base + cnt * w
+        qs = []
+        for s in slots:
+            if s != thr:
+                continue
+            q = 0
+            while bitsarr[pos + q]:
+                q += 1
+            qs.append(q)
+            pos += q + 1
+        rems = []
+        for _ in qs:
+            rems.append(get(pos, k))
+            pos += k
+        j = 0
         for i, s in enumerate(slots):
             if s == thr:
-                q = 0
-                while q < 32 and bitsarr[pos + q]:
-                    q += 1
-                if q >= 32:
-                    e = get(pos + 32, 64)
-                    pos += 96
+                if qs[j] >= 32:
+                    e = get(pos, 64)
+                    pos += 64
                 else:
-                    e = (q << k) | get(pos + q + 1, k)
-                    pos += q + 1 + k
+                    e = (qs[j] << k) | rems[j]
                 out[b * BLK + i] = thr + e
+                j += 1
             else:
                 out[b * BLK + i] = s
     return out

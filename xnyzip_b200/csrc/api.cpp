@@ -132,8 +132,10 @@ struct xnyz_ctx {
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t join_ev[kSide] = {};
-    // stage profiling (xnyz_profile / xnyz_profile_read)
+    // stage profiling (xnyz_profile / xnyz_profile_read); serial: side-stream work is issued
+    // on the context's stream so that every stage's events time that stage alone
     bool prof = false;
+    bool serial = false;
     struct ProfRec {
         const char* name;
         cudaEvent_t a, b;
@@ -249,6 +251,9 @@ xnyz_status fetch_small(xnyz_ctx* c, size_t off, size_t bytes) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return XNYZ_OK;
 }
+
+// Side stream k (the context's own stream when profiling serially).
+inline cudaStream_t side(xnyz_ctx* c, int k) { return c->serial ? c->stream : c->side[k]; }
 
 // Side stream k starts after the work queued so far on the context's stream.
 xnyz_status fork_sides(xnyz_ctx* c) {
@@ -887,33 +892,33 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     }
     TRY(fork_sides(c));
     if (ext && U) {
-        Prof pr(c, "encode_blocks", 1, 8.0 * U + ext_bits / 8.0, c->side[0]);
+        Prof pr(c, "encode_blocks", 1, 8.0 * U + ext_bits / 8.0, side(c, 0));
         launch_block_encode(at<unsigned long long>(c, cp.o_repval), U, at<uint8_t>(c, cp.o_xw), at<uint8_t>(c, cp.o_xk),
-                            at<unsigned long long>(c, cp.o_xoff), at<uint32_t>(c, o_w_xp), c->side[0]);
+                            at<unsigned long long>(c, cp.o_xoff), at<uint32_t>(c, o_w_xp), side(c, 0));
     }
     if (P && !ext) {
-        Prof pr(c, "encode_golomb_rice", 1, 8.0 * P + bits_gr / 8.0, c->side[0]);
+        Prof pr(c, "encode_golomb_rice", 1, 8.0 * P + bits_gr / 8.0, side(c, 0));
         launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
-                         SMALL_FIELD(c, tile_counters[0]), SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), c->side[0]);
+                         SMALL_FIELD(c, tile_counters[0]), SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), side(c, 0));
     }
     if (!ext && !code_rep.exp_golomb) {
-        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_rep / 8.0, c->side[1]);
+        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_rep / 8.0, side(c, 1));
         launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
                               chan(1), SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err),
-                              c->side[1]);
+                              side(c, 1));
     }
     if (!direct) {
-        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_quad / 8.0, c->side[2]);
+        Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_quad / 8.0, side(c, 2));
         launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
                               32 * words_for(bits_quad), chan(2), SMALL_FIELD(c, tile_counters[2]),
-                              SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), c->side[2]);
+                              SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), side(c, 2));
     }
     if (rle) {
-        Prof pr(c, "encode_counts", 1, 4.0 * U + bits_cnt / 8.0, c->side[3]);
+        Prof pr(c, "encode_counts", 1, 4.0 * U + bits_cnt / 8.0, side(c, 3));
         launch_count_encode(at<int32_t>(c, o_counts), U, code_cnt.exp_golomb ? code_cnt.eg_k : -1, dbits, dlen, sval,
                             sbits, slen, static_cast<uint32_t>(sparse_val.size()), at<uint32_t>(c, o_w_cn),
                             32 * words_for(bits_cnt), chan(3), SMALL_FIELD(c, tile_counters[3]),
-                            SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), c->side[3]);
+                            SMALL_FIELD(c, totals[3]), SMALL_FIELD(c, err), side(c, 3));
     }
     CUDA_TRY(cudaGetLastError());
     TRY(join_sides(c));
@@ -1384,7 +1389,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     }
     if (h.ext && U) {
         // block-coded stream: copy its parts to aligned buffers, then decode every block
-        cudaStream_t xs = c->side[0];
+        cudaStream_t xs = side(c, 0);
         const uint8_t* src = d_cont + s_gr.data_off;
         const uint64_t pad = (8 - (2 * x_nb) % 8) % 8;
         CUDA_TRY(cudaMemcpyAsync(at<uint8_t>(c, o_xw), src, x_nb, cudaMemcpyDeviceToDevice, xs));
@@ -1406,7 +1411,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                 launch_fill_u32(static_cast<uint32_t*>(j.out), j.nsym, static_cast<uint32_t>(j.fill_value), st);
             continue;
         }
-        cudaStream_t js = c->side[j.slot];
+        cudaStream_t js = side(c, j.slot);
         Prof pr(c, j.kind == kCodeGolombRice ? "decode_golomb_rice" : (j.kind == kCodeHuffman ? "decode_huffman" : "decode_exp_golomb"),
                 1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width, js);
         // Golomb-Rice tracks k + 2 entry offsets per subsequence (derived in the kernel).
@@ -2018,6 +2023,7 @@ xnyz_status xnyz_stage_sort(xnyz_ctx* c, uint64_t* dev_keys, uint32_t* dev_paylo
 xnyz_status xnyz_profile(xnyz_ctx* c, int enable) {
     if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
     c->prof = enable != 0;
+    c->serial = enable == 2;
     c->prof_recs.clear();
     c->host_ms.clear();
     c->ev_used = 0;

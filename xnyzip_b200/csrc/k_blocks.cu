@@ -1,14 +1,17 @@
 // Block-parameter coding of the repos / SFC-delta stream (the extended container).
 //
 // The stream of n u64 values is cut into blocks of 1024.  Block b is coded with a PFor slot
-// width w_b in 0..32 and a Golomb-Rice parameter k_b in 0..31:
-//   * 1024 slots of w_b bits (LSB-first): slot = v if v < 2^w - 1, else the escape 2^w - 1
-//     (w = 0: every value escapes);
-//   * then, for each escaping value in order, e = v - (2^w - 1) as a capped Golomb-Rice
-//     codeword: q = e >> k; q < 32: q ones, a zero, the k low bits of e; q >= 32: 32 ones
-//     and the 64 bits of e.
-// cost(w, k) = n_b * w + sum over escapes of (q < 32 ? q + 1 + k : 96) bits.  Blocks carry
-// their bit offset, so they encode and decode independently.
+// width w_b in 0..32 and a Golomb-Rice parameter k_b in 0..31.  Its payload (LSB-first bits,
+// starting at the block's bit offset) has four regions:
+//   S  1024 slots of w_b bits: slot = v if v < 2^w - 1, else the escape 2^w - 1 (w = 0:
+//      every value escapes);
+//   U  for each escaping value in order, with e = v - (2^w - 1) and q = e >> k: min(q, 32)
+//      one bits and a zero (q >= 32 marks a capped escape);
+//   R  for each escaping value, the k low bits of e;
+//   X  for each capped escape, the 64 bits of e.
+// cost(w, k) = n_b * w + sum over escapes of (min(q, 32) + 1 + k + (q >= 32 ? 64 : 0)) bits.
+// Blocks carry their bit offset, so they encode and decode independently, and every region
+// decodes warp-parallel (escape j's unary part lies between the (j-1)-th and j-th zero of U).
 //
 // Kernels (one warp per block): features for the parameter predictor, the exhaustive search
 // over all 33 x 32 (w, k) pairs (training labels, fallback and judge), the cost of given
@@ -29,7 +32,7 @@ __device__ __forceinline__ u64 escape_threshold(int w) { return (1ull << w) - 1u
 
 __device__ __forceinline__ u32 esc_len(u64 e, int k) {
     const u64 q = e >> k;
-    return q < 32 ? (u32)q + 1u + (u32)k : 96u;
+    return q < 32 ? (u32)q + 1u + (u32)k : 97u + (u32)k;
 }
 
 __device__ __forceinline__ u32 block_count(u64 n, u64 b) {
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(32 * WARPS) features_kernel(const u64* __restr
 
 // ------------------------------------------------------------------ search --------------
 // For each w: escapes e with L = bitlen(e) contribute (1 + k) for k >= L, (e >> k) + 1 + k
-// for L - 5 <= k < L, and 96 for k < L - 5.  Lanes accumulate the exact middle terms in
+// for L - 5 <= k < L, and 97 + k for k < L - 5.  Lanes accumulate the exact middle terms in
 // their own shared-memory row and the two others through a histogram of L.
 struct SearchShared {
     u32 acc[WARPS][32][33];   // [warp][lane][k] exact middle terms
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(32 * WARPS) search_kernel(const u64* __restric
                 if (L <= k) le += h;
                 else if (L > k + 5) gt += h;
             }
-            sh.cost[wi][w][k] = cnt * (u32)w + s + le * (1u + (u32)k) + gt * 96u;
+            sh.cost[wi][w][k] = cnt * (u32)w + s + le * (1u + (u32)k) + gt * (97u + (u32)k);
         }
         __syncwarp();
     }
@@ -192,6 +195,18 @@ __device__ __forceinline__ void or_bits(u32* words, u64 pos, u64 val, u32 nbits)
     if (o + nbits > 64) atomicOr(&words[wk + 2], (u32)((lo >> (32 - o)) >> 32));
 }
 
+// warp exclusive prefix sum; *total receives the sum over the warp
+__device__ __forceinline__ u32 warp_excl(u32 v, u32* total) {
+    const int lane = threadIdx.x & 31;
+    u32 incl = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const u32 o = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += o;
+    }
+    *total = __shfl_sync(kFullMask, incl, 31);
+    return incl - v;
+}
+
 // Encoder: block offsets (exclusive prefix of the costs, bits) are given.  The payload must
 // be zeroed.
 __global__ void __launch_bounds__(32 * WARPS) encode_kernel(const u64* __restrict__ v, u64 n, u64 nblk,
@@ -204,46 +219,56 @@ __global__ void __launch_bounds__(32 * WARPS) encode_kernel(const u64* __restric
     const int w = min((int)win[b], 32), k = min((int)kin[b], 31);
     const u64 thr = escape_threshold(w);
     const u64* p = v + b * BLK;
-    const u64 base = offs[b];
-    u64 epos = base + (u64)cnt * (u64)w;  // escape region
+    // pass 1: sizes of the U region and escape counts
+    u32 ubits = 0, nesc = 0;
+    for (u32 i = lane; i < cnt; i += 32) {
+        const u64 x = p[i];
+        if (x >= thr) {
+            const u64 q = (x - thr) >> k;
+            ubits += (u32)min(q, (u64)32) + 1u;
+            ++nesc;
+        }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        ubits += __shfl_xor_sync(kFullMask, ubits, d);
+        nesc += __shfl_xor_sync(kFullMask, nesc, d);
+    }
+    const u64 s0 = offs[b], u0 = s0 + (u64)cnt * (u64)w, r0 = u0 + ubits, x0 = r0 + (u64)nesc * (u64)k;
+    // pass 2: write the regions
+    u64 upos = u0;
+    u32 erank = 0, crank = 0;
     for (u32 i0 = 0; i0 < cnt; i0 += 32) {
         const u32 i = i0 + lane;
         const bool ok = i < cnt;
         const u64 x = ok ? p[i] : 0ull;
         const bool esc = ok && x >= thr;
-        if (ok) or_bits(payload, base + (u64)i * (u64)w, esc ? thr : x, (u32)w);
-        const u32 len = esc ? esc_len(x - thr, k) : 0u;
-        // warp exclusive prefix of the escape lengths
-        u32 incl = len;
-        for (int d = 1; d < 32; d <<= 1) {
-            const u32 o = __shfl_up_sync(kFullMask, incl, d);
-            if (lane >= d) incl += o;
-        }
-        const u32 tot = __shfl_sync(kFullMask, incl, 31);
+        if (ok) or_bits(payload, s0 + (u64)i * (u64)w, esc ? thr : x, (u32)w);
+        const u64 e = esc ? x - thr : 0ull;
+        const u64 q = e >> k;
+        const bool capped = esc && q >= 32;
+        const u32 ulen = esc ? (u32)min(q, (u64)32) + 1u : 0u;
+        u32 utot, etot, ctot;
+        const u32 uoff = warp_excl(ulen, &utot);
+        const u32 eoff = warp_excl(esc ? 1u : 0u, &etot);
+        const u32 coff = warp_excl(capped ? 1u : 0u, &ctot);
         if (esc) {
-            const u64 e = x - thr;
-            const u64 pos = epos + (incl - len);
-            const u64 q = e >> k;
-            if (q < 32) {
-                // q ones, a zero, then k bits
-                or_bits(payload, pos, (1ull << q) - 1ull, (u32)q + 1u);
-                or_bits(payload, pos + q + 1, e, (u32)k);
-            } else {
-                or_bits(payload, pos, 0xffffffffull, 32u);
-                or_bits(payload, pos + 32, e, 64u);
-            }
+            or_bits(payload, upos + uoff, (1ull << (ulen - 1)) - 1ull, ulen);  // ulen-1 ones, a zero
+            or_bits(payload, r0 + (u64)(erank + eoff) * (u64)k, e, (u32)k);
+            if (capped) or_bits(payload, x0 + (u64)(crank + coff) * 64ull, e, 64u);
         }
-        epos += tot;
+        upos += utot;
+        erank += etot;
+        crank += ctot;
     }
 }
 
-// Decoder: one warp per block.  Lanes read the slots; lane 0 then decodes the escape
-// codewords in order into shared memory.
+// Decoder: one warp per block.  Lanes read the slots, locate the zeros of the U region by a
+// warp scan of its words, then read each escape's remainder and capped value.
 __global__ void __launch_bounds__(32 * WARPS) decode_kernel(const u32* __restrict__ payload, u64 payload_bits, u64 n,
                                                             u64 nblk, const u8* __restrict__ win,
                                                             const u8* __restrict__ kin, const u64* __restrict__ offs,
                                                             u64* __restrict__ out, u32* err) {
-    __shared__ u64 sesc[WARPS][BLK];
+    __shared__ u32 szero[WARPS][BLK];  // position of the j-th zero of U, relative to U's start
     const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u64 b = (u64)blockIdx.x * WARPS + wi;
     if (b >= nblk) return;
@@ -263,6 +288,7 @@ __global__ void __launch_bounds__(32 * WARPS) decode_kernel(const u32* __restric
         const u64 lo = (u64)word(i) | ((u64)word(i + 1) << 32);
         return o ? ((lo >> o) | ((u64)word(i + 2) << (64 - o))) : lo;
     };
+    // slots
     u32 esc_mask[PER_LANE];
     u32 nesc = 0;
     u64 xs[PER_LANE];
@@ -276,36 +302,55 @@ __global__ void __launch_bounds__(32 * WARPS) decode_kernel(const u32* __restric
         esc_mask[r] = __ballot_sync(kFullMask, esc);
         nesc += __popc(esc_mask[r]);
     }
-    if (lane == 0) {
-        u64 pos = base + (u64)cnt * (u64)w;
-        for (u32 j = 0; j < nesc; ++j) {
-            const u64 bits = peek64(pos);
-            u32 q = bits == ~0ull ? 64u : (u32)(__ffsll((long long)~bits) - 1);
-            u64 e;
-            if (q >= 32) {
-                e = peek64(pos + 32);
-                pos += 96;
-            } else {
-                e = ((u64)q << k) | (k ? (peek64(pos + q + 1) & ((1ull << k) - 1ull)) : 0ull);
-                pos += (u64)q + 1 + (u64)k;
-            }
-            sesc[wi][j] = e;
+    const u64 u0 = base + (u64)cnt * (u64)w;
+    // zeros of U: 32-bit chunks (lane j: bits u0 + 32 * (32 c + j) ...), until nesc found
+    u32 found = 0;
+    for (u64 c0 = 0; found < nesc; c0 += 32 * 32) {
+        const u64 pos = u0 + c0 + 32ull * lane;
+        const u32 bits = pos < payload_bits ? (u32)peek64(pos) : 0u;
+        u32 zeros = ~bits;
+        if (pos + 32 > payload_bits) zeros &= pos >= payload_bits ? 0u : ((1u << (payload_bits - pos)) - 1u);
+        u32 ztot;
+        const u32 zoff = warp_excl((u32)__popc(zeros), &ztot);
+        u32 j = found + zoff;
+        while (zeros && j < nesc) {
+            const int bpos = __ffs((int)zeros) - 1;
+            zeros &= zeros - 1;
+            szero[wi][j++] = (u32)(c0 + 32ull * lane + (u64)bpos);
         }
-        if (pos > payload_bits) atomicOr(err, kErrBadStream);
+        found += ztot;
+        if (c0 > 33ull * BLK + 64) break;  // more bits than any block's U region: corrupt
     }
     __syncwarp();
-    u32 before = 0;
+    if (found < nesc) {
+        if (lane == 0) atomicOr(err, kErrBadStream);
+        return;
+    }
+    const u64 r0 = nesc ? u0 + szero[wi][nesc - 1] + 1 : u0;
+    const u64 x0 = r0 + (u64)nesc * (u64)k;
+    u32 before = 0, cbefore = 0;
 #pragma unroll
     for (int r = 0; r < PER_LANE; ++r) {
         const u32 i = (u32)r * 32 + lane;
         const u32 m = esc_mask[r];
-        if (i < cnt) {
-            u64 x = xs[r];
-            if ((m >> lane) & 1u) x = thr + sesc[wi][before + __popc(m & ((1u << lane) - 1u))];
-            out[b * BLK + i] = x;
+        const bool esc = (m >> lane) & 1u;
+        u64 x = xs[r];
+        u32 q = 0;
+        if (esc) {
+            const u32 j = before + __popc(m & ((1u << lane) - 1u));
+            const u32 zj = szero[wi][j], zp = j ? szero[wi][j - 1] + 1 : 0u;
+            q = zj - zp;
+            const u64 rem = k ? (peek64(r0 + (u64)j * (u64)k) & ((1ull << k) - 1ull)) : 0ull;
+            x = thr + (((u64)q << k) | rem);
         }
+        const bool capped = esc && q >= 32;
+        const u32 cm = __ballot_sync(kFullMask, capped);
+        if (capped) x = thr + peek64(x0 + 64ull * (cbefore + __popc(cm & ((1u << lane) - 1u))));
+        if (i < cnt) out[b * BLK + i] = x;
         before += __popc(m);
+        cbefore += __popc(cm);
     }
+    if (lane == 0 && x0 + 64ull * cbefore > payload_bits) atomicOr(err, kErrBadStream);
 }
 
 // Exclusive prefix sum of the block costs (bits) -> offsets, single CTA (block counts are
