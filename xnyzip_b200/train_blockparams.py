@@ -43,15 +43,19 @@ from .synthetic_gpu import gen_spheres, gen_terrain, gen_uniform  # noqa: E402
 
 
 def workloads(seed):
-    """(generator, n, quantizer, l2, hilbert, rle) of one seed: the plain-method grid."""
+    """(generator, n, quantizer, l2, hilbert, rle) of one seed: the plain-method grid.  Point
+    density shapes the deltas, so terrain alternates between 16M and 64M points (the
+    terrain workload's size) and spheres between 16M and 48M."""
     out = [("uniform", 1_000_000, 1, 0.05, 0, 1)]
+    nt = 64_000_000 if seed % 2 == 0 else 16_000_000
+    ns = 48_000_000 if seed % 2 == 0 else 16_000_000
     for q in (1, 0):
         for l2 in (0.001, 0.01, 0.1):
-            out.append(("terrain", 16_000_000, q, l2, 1, 1))
-            out.append(("terrain", 16_000_000, q, l2, 0, 0))
-    out.append(("spheres", 16_000_000, 1, 0.5, 0, 0))
-    out.append(("spheres", 16_000_000, 1, 0.5, 0, 1))
-    out.append(("spheres", 16_000_000, 0, 0.05, 1, 1))
+            out.append(("terrain", nt, q, l2, 1, 1))
+            out.append(("terrain", nt, q, l2, 0, 0))
+    out.append(("spheres", ns, 1, 0.5, 0, 0))
+    out.append(("spheres", ns, 1, 0.5, 0, 1))
+    out.append(("spheres", ns, 0, 0.05, 1, 1))
     # small clouds fall into direct mode (the SFC-delta stream)
     out.append(("spheres_small", 400_000, 1, 0.1, 1, 1))
     out.append(("terrain_small", 400_000, 0, 0.1, 0, 1))
