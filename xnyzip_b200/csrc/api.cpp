@@ -1539,6 +1539,11 @@ xnyz_status decompress_run(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, con
 }  // namespace
 
 namespace xnyz {
+// An entry point reports only its own CUDA errors: a sticky error left on this thread by an
+// earlier call outside the library (or by a call whose failure was already reported) is
+// cleared first.
+void clear_stale_cuda_error() { (void)cudaGetLastError(); }
+
 // Sets the calling thread's xnyz_last_error() message (used by the batch pool).
 xnyz_status set_last_error(xnyz_status s, const std::string& msg) { return fail(s, msg); }
 }  // namespace xnyz
@@ -1550,6 +1555,7 @@ const char* xnyz_last_error(void) { return g_last_error.c_str(); }
 const char* xnyz_version(void) { return "xnyzip-b200 0.1 (sm_100a)"; }
 
 xnyz_status xnyz_create(xnyz_ctx** out, int device, void* stream) {
+    clear_stale_cuda_error();
     if (!out) return fail(XNYZ_ERR_INVALID_ARG, "null context pointer");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(XNYZ_ERR_NO_DEVICE, "no CUDA device");
@@ -1606,10 +1612,12 @@ xnyz_status xnyz_destroy(xnyz_ctx* c) {
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
+    (void)cudaGetLastError();  // teardown is best effort: leave no sticky error behind
     return XNYZ_OK;
 }
 
 xnyz_status xnyz_trim(xnyz_ctx* c) {
+    clear_stale_cuda_error();
     if (!c) return fail(XNYZ_ERR_INVALID_ARG, "null context");
     cudaSetDevice(c->device);
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1643,6 +1651,7 @@ void xnyz_free(void* p) { std::free(p); }
 xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_device, const xnyz_params* params,
                           int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order,
                           xnyz_compress_info* info) {
+    clear_stale_cuda_error();
     if (!c || !xyz || !params || !out || !out_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(c->device));
     if (use_zstd) {
@@ -1710,6 +1719,7 @@ xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_
 
 xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, const xnyz_params* params,
                                  const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info) {
+    clear_stale_cuda_error();
     if (!c || !xyz || !params || !dev_container || !container_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
@@ -1782,6 +1792,7 @@ xnyz_status decompress_host_input(xnyz_ctx* c, const uint8_t* in, uint64_t in_le
 
 xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
                             float l2_bound, int rle, float** xyz, uint64_t* n) {
+    clear_stale_cuda_error();
     if (!xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     float* d_out = nullptr;
     uint64_t nout = 0;
@@ -1807,6 +1818,7 @@ xnyz_status xnyz_decompress(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int
 
 xnyz_status xnyz_decompress_into(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
                                  float l2_bound, int rle, float* xyz, uint64_t capacity, uint64_t* n) {
+    clear_stale_cuda_error();
     if (!xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     float* d_out = nullptr;
     uint64_t nout = 0;
@@ -1821,6 +1833,7 @@ xnyz_status xnyz_decompress_into(xnyz_ctx* c, const uint8_t* in, uint64_t in_len
 
 xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, uint64_t len, int quantizer,
                                    float l2_bound, int rle, const float** dev_xyz, uint64_t* n) {
+    clear_stale_cuda_error();
     if (!c || !dev_container || !dev_xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
         return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
@@ -1867,6 +1880,7 @@ xnyz_status xnyz_set_block_mode(xnyz_ctx* c, int mode) {
 uint64_t xnyz_model_param_count(void) { return kParamCount; }
 
 xnyz_status xnyz_set_model(xnyz_ctx* c, const float* params, uint64_t count, float fallback_confidence) {
+    clear_stale_cuda_error();
     if (!c || !params) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     if (count != static_cast<uint64_t>(kParamCount))
         return fail(XNYZ_ERR_INVALID_ARG, "expected " + std::to_string(kParamCount) + " parameters");
@@ -1888,6 +1902,7 @@ xnyz_status xnyz_last_block_info(xnyz_ctx* c, xnyz_block_info* info) {
 
 xnyz_status xnyz_stage_repos(xnyz_ctx* c, const float* dev_xyz, uint64_t n, const xnyz_params* params,
                              uint64_t* dev_out, uint64_t cap, uint64_t* count) {
+    clear_stale_cuda_error();
     if (!c || !dev_xyz || !params || !count || (cap && !dev_out)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     const int mode = c->block_mode;
     c->block_mode = XNYZ_BLOCKS_GLOBAL;
@@ -1904,12 +1919,14 @@ xnyz_status xnyz_stage_repos(xnyz_ctx* c, const float* dev_xyz, uint64_t n, cons
 }
 
 xnyz_status xnyz_block_features(const uint64_t* v, uint64_t n, float* feats, void* stream) {
+    clear_stale_cuda_error();
     if (n && (!v || !feats)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     launch_block_features(reinterpret_cast<const unsigned long long*>(v), n, feats, static_cast<cudaStream_t>(stream));
     CUDA_TRY(cudaGetLastError());
     return XNYZ_OK;
 }
 xnyz_status xnyz_block_search(const uint64_t* v, uint64_t n, uint8_t* w, uint8_t* k, uint32_t* cost, void* stream) {
+    clear_stale_cuda_error();
     if (n && (!v || !w || !k)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     launch_block_search(reinterpret_cast<const unsigned long long*>(v), n, nullptr, w, k, cost,
                         static_cast<cudaStream_t>(stream));
@@ -1918,6 +1935,7 @@ xnyz_status xnyz_block_search(const uint64_t* v, uint64_t n, uint8_t* w, uint8_t
 }
 xnyz_status xnyz_block_cost(const uint64_t* v, uint64_t n, const uint8_t* w, const uint8_t* k, uint32_t* cost,
                             void* stream) {
+    clear_stale_cuda_error();
     if (n && (!v || !w || !k || !cost)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     launch_block_cost(reinterpret_cast<const unsigned long long*>(v), n, w, k, cost, static_cast<cudaStream_t>(stream));
     CUDA_TRY(cudaGetLastError());
@@ -1925,6 +1943,7 @@ xnyz_status xnyz_block_cost(const uint64_t* v, uint64_t n, const uint8_t* w, con
 }
 xnyz_status xnyz_mlp_forward(const float* prm, const float* feats, uint64_t count, uint8_t* w, uint8_t* k, float* conf,
                              float* logits, void* stream) {
+    clear_stale_cuda_error();
     if (count && (!prm || !feats || !w || !k)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     launch_mlp_forward(prm, feats, count, w, k, conf, logits, static_cast<cudaStream_t>(stream));
     CUDA_TRY(cudaGetLastError());
@@ -1934,6 +1953,7 @@ uint64_t xnyz_mlp_gather_floats(uint64_t count) { return mlp_gather_floats(count
 xnyz_status xnyz_mlp_train_batch(const float* prm, const float* feats, const uint8_t* w, const uint8_t* k,
                                  const uint32_t* idx, uint64_t first, uint64_t count, float scale, float* grad,
                                  float* loss, float* gather, void* stream) {
+    clear_stale_cuda_error();
     if (count && (!prm || !feats || !w || !k || !grad || !loss || !gather))
         return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     launch_mlp_train(prm, feats, w, k, idx, first, count, scale, grad, loss, gather, static_cast<cudaStream_t>(stream));
@@ -1941,6 +1961,7 @@ xnyz_status xnyz_mlp_train_batch(const float* prm, const float* feats, const uin
     return XNYZ_OK;
 }
 xnyz_status xnyz_mlp_adam(float* prm, float* grad, float* m, float* v, float lr, int step, void* stream) {
+    clear_stale_cuda_error();
     if (!prm || !grad || !m || !v || step < 1) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
     launch_mlp_adam(prm, grad, m, v, lr, step, static_cast<cudaStream_t>(stream));
     CUDA_TRY(cudaGetLastError());
@@ -1950,6 +1971,7 @@ xnyz_status xnyz_mlp_adam(float* prm, float* grad, float* m, float* v, float lr,
 // ---- stage entry points -------------------------------------------------------------------
 xnyz_status xnyz_stage_quantize(xnyz_ctx* c, const float* dev_xyz, uint64_t n, int quantizer, float l2_bound,
                                 float* offset3, int32_t* dev_cells) {
+    clear_stale_cuda_error();
     if (!c || !dev_xyz || !offset3 || !dev_cells || n == 0) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(c->device));
     const QuantParams q = make_quant(quantizer, l2_bound);
@@ -1971,6 +1993,7 @@ xnyz_status xnyz_stage_quantize(xnyz_ctx* c, const float* dev_xyz, uint64_t n, i
 
 xnyz_status xnyz_stage_recover(xnyz_ctx* c, const int32_t* dev_cells, uint64_t n, int quantizer, float l2_bound,
                                const float* offset3, float* dev_xyz) {
+    clear_stale_cuda_error();
     if (!c || !dev_cells || !offset3 || !dev_xyz) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(c->device));
     for (int a = 0; a < 3; ++a) c->h_small->offset_in[a] = offset3[a];
@@ -1983,6 +2006,7 @@ xnyz_status xnyz_stage_recover(xnyz_ctx* c, const int32_t* dev_cells, uint64_t n
 
 xnyz_status xnyz_stage_hilbert(xnyz_ctx* c, const uint64_t* dev_in, uint64_t n, unsigned iteration, int inverse,
                                uint64_t* dev_out) {
+    clear_stale_cuda_error();
     if (!c || !dev_in || !dev_out) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
     if (iteration > 20) return fail(XNYZ_ERR_UNSUPPORTED, "iteration above 20");
     CUDA_TRY(cudaSetDevice(c->device));
@@ -1997,6 +2021,7 @@ xnyz_status xnyz_stage_hilbert(xnyz_ctx* c, const uint64_t* dev_in, uint64_t n, 
 }
 
 xnyz_status xnyz_stage_sort(xnyz_ctx* c, uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits) {
+    clear_stale_cuda_error();
     if (!c || !dev_keys || key_bits < 0 || key_bits > 64) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
     if (n >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 keys");
     CUDA_TRY(cudaSetDevice(c->device));
@@ -2031,6 +2056,7 @@ xnyz_status xnyz_profile(xnyz_ctx* c, int enable) {
 }
 
 xnyz_status xnyz_profile_read(xnyz_ctx* c, char* json, uint64_t cap, uint64_t* len) {
+    clear_stale_cuda_error();
     if (!c || !len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
