@@ -76,27 +76,22 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     }
     __syncthreads();
 
-    // Pass A: classify my 16 consecutive elements.
-    u64 val[kItems];  // repos / sfc delta
-    u64 idv[kItems];  // block id (block mode)
-    u32 fl[kItems];   // bit0 head, bit1 patch, bit2 new block, bits 8..15 quad delta
-    u32 h = 0, p = 0, b = 0;
-#pragma unroll
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = (u32)tid * kItems + i;
-        fl[i] = 0;
-        val[i] = 0;
-        idv[i] = 0;
-        if (e >= cnt) continue;
+    // Element e of the tile: flags (bit0 head, bit1 patch, bit2 new block, bits 8..15 quad
+    // delta), repos / SFC delta and block id.  Computed in pass A for the counts and again in
+    // pass B from the staged keys (cheaper than holding 16 of each in registers).
+    auto classify = [&](u32 e, u64& val, u64& idv) -> u32 {
+        val = 0;
+        idv = 0;
+        if (e >= cnt) return 0u;
         const u64 j = base + e;
         const u64 k = sk[1 + e], kp = sk[e];
         const bool head = !rle || j == 0 || k != kp;
-        if (!head) continue;
+        if (!head) return 0u;
         u32 f = 1u;
         if (DIRECT) {
             const u64 s = direct_key_sfc(k, dkp);
             const u64 d = j == 0 ? s : s - direct_key_sfc(kp, dkp);
-            val[i] = d;
+            val = d;
             if (d > 254u) f |= 2u;
         } else {
             u64 id, idp = 0;
@@ -117,13 +112,19 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
                 qd = 0;
                 r = (u64)sfc - (u64)sfcp;
             }
-            val[i] = r;
-            idv[i] = id;
+            val = r;
+            idv = id;
             if (r > 254u) f |= 2u;
             f |= (qd & 0xffu) << 8;
         }
-        fl[i] = f;
-        h += 1;
+        return f;
+    };
+    // Pass A: count heads, patches and new blocks of my 16 consecutive elements.
+    u32 h = 0, p = 0, b = 0;
+    for (int i = 0; i < kItems; ++i) {
+        u64 v, id;
+        const u32 f = classify((u32)tid * kItems + i, v, id);
+        h += f & 1u;
         p += (f >> 1) & 1u;
         b += (f >> 2) & 1u;
     }
@@ -147,23 +148,23 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     u64 pp = sbase[1] + ((ex >> 21) & ((1ull << 21) - 1));
     u64 bb = sbase[2] + ((ex >> 42) & ((1ull << 21) - 1));
     u64 mysum = 0;
-#pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        const u32 f = fl[i];
+        u64 vi, idi;
+        const u32 f = classify((u32)tid * kItems + i, vi, idi);
         const bool head = f & 1u;
         const bool patch = (f >> 1) & 1u;
-        const u32 sym = head ? (patch ? 0u : (u32)val[i] + 1u) : 0u;
+        const u32 sym = head ? (patch ? 0u : (u32)vi + 1u) : 0u;
         const u32 qsym = ((f >> 8) & 0xffu) + 1u;
         if (head) {
             out.rep_sym[uu] = (u8)sym;
-            if (out.rep_val) out.rep_val[uu] = val[i];
+            if (out.rep_val) out.rep_val[uu] = vi;
             if (!DIRECT) out.quad_sym[uu] = (u8)qsym;
             if (patch) {
-                out.patches[pp] = val[i];
-                mysum += val[i];
+                out.patches[pp] = vi;
+                mysum += vi;
             }
             if (!DIRECT && ((f >> 2) & 1u)) {
-                out.blk_id[bb] = idv[i];
+                out.blk_id[bb] = idi;
                 out.blk_unit[bb] = (u32)uu;
             }
             if (rle) out.unit_pos[uu] = (u32)(base + (u32)tid * kItems + i);
