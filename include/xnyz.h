@@ -177,6 +177,29 @@ xnyz_status xnyz_batch_decompress(xnyz_batch* batch, uint64_t count, const uint8
                                   int is_zstd, const int* quantizer, const float* l2_bound, const int* rle,
                                   float* const* xyz, const uint64_t* capacity, uint64_t* n, xnyz_status* item_status);
 
+/* ---- distributed-RLE cell tables ------------------------------------------------------------ */
+
+/* XnYZip::BlockCompressorRLE<float>::encode_cells_with_counts (composer/block_compressor_rle.hpp:341-470):
+ * n unique lattice cells (int32 xyz triples) with their counts, the GLOBAL ranges and offset,
+ * Hilbert (1) or Morton (0) curve -> a -rle container in block mode (zstd frame when use_zstd).
+ * Cells must lie in [0, range] (z may be -1, the truncated-octahedron edge cell); counts
+ * travel in the container's cell order.  Inputs in device memory when cells_is_device. */
+xnyz_status xnyz_encode_cells(xnyz_ctx* ctx, const int32_t* cells, const int32_t* counts, uint64_t n,
+                              int cells_is_device, const int32_t* ranges, const float* offset, int hilbert,
+                              int use_zstd, uint8_t** out, uint64_t* out_len);
+/* XnYZip::BlockDecompressorRLE<float>::decompress_to_cells (composer/block_decompressor_rle.hpp:230-335):
+ * a -rle block-mode container (zstd frame when is_zstd) -> its cells and counts in container
+ * order (malloc'd, release with xnyz_free), the offset, ranges and curve flag.  A direct-mode
+ * container is rejected with XNYZ_ERR_BAD_STREAM, as the reference throws. */
+xnyz_status xnyz_decompress_to_cells(xnyz_ctx* ctx, const uint8_t* in, uint64_t in_len, int is_zstd,
+                                     int32_t** cells, int32_t** counts, uint64_t* n, float* offset,
+                                     int32_t* ranges, int* hilbert);
+/* XnYZip::BlockDecompressorRLE<float>::expand_cells_to_points (composer/block_decompressor_rle.hpp:339-358):
+ * every cell repeated counts[i] times, recovered by the quantizer and unshifted by offset
+ * (host arrays in, a malloc'd array of 3 * n_points floats out). */
+xnyz_status xnyz_expand_cells(xnyz_ctx* ctx, const int32_t* cells, const int32_t* counts, uint64_t n, int quantizer,
+                              float l2_bound, const float* offset, float** xyz, uint64_t* n_points);
+
 /* ---- extended container: block parameters of the repos / SFC-delta stream ------------------ *
  * No counterpart in the reference (it codes this stream with one Golomb-Rice k for the
  * patches and a Huffman code for the PFor symbols, block_compressor.hpp:122-136,174-190).

@@ -184,6 +184,55 @@ class Reference(Oracle):
             raise RuntimeError("ref_decompress failed")
         return self.take(out, 3 * n.value, np.float32).reshape(-1, 3)
 
+    def encode_cells(self, cells, counts, ranges, offset, hilbert, quantizer="to", l2=0.05):
+        """BlockCompressorRLE::encode_cells_with_counts: the zstd frame."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+        off = np.ascontiguousarray(offset, dtype=np.float32)
+        out, ln = _u8p(), C.c_uint64()
+        rc = self.fn("encode_cells", [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_int, C.c_int, C.c_float, C.POINTER(_u8p), C.POINTER(C.c_uint64)])(
+            _buf(cells), _buf(counts), cells.shape[0], int(ranges[0]), int(ranges[1]), int(ranges[2]), _buf(off),
+            int(hilbert), QUANT.get(quantizer, quantizer), l2, C.byref(out), C.byref(ln))
+        if rc:
+            raise RuntimeError("ref_encode_cells failed")
+        return self.take(out, ln.value).tobytes()
+
+    def decompress_to_cells(self, buf, quantizer="to", l2=0.05):
+        """BlockDecompressorRLE::decompress_to_cells: (cells, counts, offset, ranges, hilbert)."""
+        b = np.frombuffer(buf, dtype=np.uint8)
+        _i32p = C.POINTER(C.c_int32)
+        cp, kp, n = _i32p(), _i32p(), C.c_uint64()
+        off = np.zeros(3, np.float32)
+        rng = np.zeros(3, np.int32)
+        hil = C.c_int()
+        rc = self.fn("decompress_to_cells", [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.POINTER(_i32p),
+                                             C.POINTER(_i32p), C.POINTER(C.c_uint64), C.c_void_p, C.c_void_p,
+                                             C.POINTER(C.c_int)])(
+            _buf(b), len(buf), QUANT.get(quantizer, quantizer), l2, C.byref(cp), C.byref(kp), C.byref(n), _buf(off),
+            _buf(rng), C.byref(hil))
+        if rc:
+            raise RuntimeError("ref_decompress_to_cells failed")
+        cells = np.ctypeslib.as_array(cp, shape=(3 * n.value,)).copy().reshape(-1, 3)
+        counts = np.ctypeslib.as_array(kp, shape=(n.value,)).copy()
+        self.fn("free", [C.c_void_p], None)(C.cast(cp, C.c_void_p))
+        self.fn("free", [C.c_void_p], None)(C.cast(kp, C.c_void_p))
+        return cells, counts, off, rng, bool(hil.value)
+
+    def expand_cells(self, cells, counts, offset, quantizer="to", l2=0.05):
+        """BlockDecompressorRLE::expand_cells_to_points."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+        off = np.ascontiguousarray(offset, dtype=np.float32)
+        out, n = _f32p(), C.c_uint64()
+        rc = self.fn("expand_cells", [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_float,
+                                      C.POINTER(_f32p), C.POINTER(C.c_uint64)])(
+            _buf(cells), _buf(counts), cells.shape[0], _buf(off), QUANT.get(quantizer, quantizer), l2, C.byref(out),
+            C.byref(n))
+        if rc:
+            raise RuntimeError("ref_expand_cells failed")
+        return self.take(out, 3 * n.value, np.float32).reshape(-1, 3)
+
     def unzstd(self, buf):
         b = np.frombuffer(buf, dtype=np.uint8)
         out, ln = _u8p(), C.c_uint64()

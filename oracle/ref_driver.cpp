@@ -325,4 +325,72 @@ int ref_bitpack(const uint64_t* data, uint64_t n, uint8_t** meta, uint64_t* meta
     }
 }
 
+// Distributed-RLE cell API (composer/block_compressor_rle.hpp:341-470,
+// composer/block_decompressor_rle.hpp:230-358): cells are int32 xyz triples.
+int ref_encode_cells(const int32_t* cells, const int32_t* counts, uint64_t n, int rx, int ry, int rz,
+                     const float* offset3, int hilbert, int quantizer, float l2, uint8_t** out, uint64_t* out_len) {
+    try {
+        std::vector<Eigen::RowVector3i> c;
+        c.reserve(n);
+        for (uint64_t i = 0; i < n; ++i) c.emplace_back(cells[3 * i], cells[3 * i + 1], cells[3 * i + 2]);
+        std::vector<int> k(counts, counts + n);
+        XnYZip::BlockCompressorRLE<float> enc(qtype(quantizer), l2);
+        auto bytes = enc.encode_cells_with_counts(c, k, rx, ry, rz, P3(offset3[0], offset3[1], offset3[2]), hilbert != 0);
+        *out = dup_bytes(bytes, out_len);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_encode_cells: %s\n", e.what());
+        return 1;
+    }
+}
+
+int ref_decompress_to_cells(const uint8_t* buf, uint64_t len, int quantizer, float l2, int32_t** cells_out,
+                            int32_t** counts_out, uint64_t* n_out, float* offset3, int32_t* ranges3, int* hilbert) {
+    try {
+        std::vector<uint8_t> bytes(buf, buf + len);
+        XnYZip::BlockDecompressorRLE<float> d(qtype(quantizer), l2);
+        auto t = d.decompress_to_cells(bytes);
+        *n_out = t.cells.size();
+        int32_t* c = static_cast<int32_t*>(std::malloc(t.cells.size() * 12 + 4));
+        int32_t* k = static_cast<int32_t*>(std::malloc(t.counts.size() * 4 + 4));
+        for (size_t i = 0; i < t.cells.size(); ++i)
+            for (int a = 0; a < 3; ++a) c[3 * i + a] = t.cells[i][a];
+        for (size_t i = 0; i < t.counts.size(); ++i) k[i] = t.counts[i];
+        *cells_out = c;
+        *counts_out = k;
+        for (int a = 0; a < 3; ++a) offset3[a] = t.offset[a];
+        ranges3[0] = t.range_x;
+        ranges3[1] = t.range_y;
+        ranges3[2] = t.range_z;
+        *hilbert = t.is_hilbert;
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_decompress_to_cells: %s\n", e.what());
+        return 1;
+    }
+}
+
+int ref_expand_cells(const int32_t* cells, const int32_t* counts, uint64_t n, const float* offset3, int quantizer,
+                     float l2, float** xyz_out, uint64_t* n_out) {
+    try {
+        XnYZip::BlockDecompressorRLE<float> d(qtype(quantizer), l2);
+        XnYZip::BlockDecompressorRLE<float>::DecodedCellTable t;
+        for (uint64_t i = 0; i < n; ++i) {
+            t.cells.emplace_back(cells[3 * i], cells[3 * i + 1], cells[3 * i + 2]);
+            t.counts.push_back(counts[i]);
+        }
+        t.offset = P3(offset3[0], offset3[1], offset3[2]);
+        auto pts = d.expand_cells_to_points(t);
+        *n_out = pts.size();
+        float* o = static_cast<float*>(std::malloc(pts.size() * 12 + 4));
+        for (size_t i = 0; i < pts.size(); ++i)
+            for (int a = 0; a < 3; ++a) o[3 * i + a] = pts[i][a];
+        *xyz_out = o;
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_expand_cells: %s\n", e.what());
+        return 1;
+    }
+}
+
 }  // extern "C"

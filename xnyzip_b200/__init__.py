@@ -155,6 +155,56 @@ class Context:
                               C.byref(cnt)))
         return cnt.value
 
+    # -- distributed-RLE cell tables --------------------------------------------------
+    def encode_cells(self, cells, counts, ranges, offset, hilbert: bool, use_zstd: bool = True) -> bytes:
+        """encode_cells_with_counts: int32 (n, 3) cells, int32 counts, global ranges / offset."""
+        cl = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        ct = np.ascontiguousarray(counts, dtype=np.int32)
+        rg = np.ascontiguousarray(ranges, dtype=np.int32)
+        of = np.ascontiguousarray(offset, dtype=np.float32)
+        out = C.POINTER(C.c_uint8)()
+        ln = C.c_uint64()
+        N.check(N.encode_cells(self.handle, cl.ctypes.data_as(C.c_void_p), ct.ctypes.data_as(C.c_void_p), cl.shape[0],
+                               0, rg.ctypes.data_as(C.c_void_p), of.ctypes.data_as(C.c_void_p), int(bool(hilbert)),
+                               int(use_zstd), C.byref(out), C.byref(ln)))
+        try:
+            return C.string_at(out, ln.value)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+
+    def decompress_to_cells(self, data: bytes, is_zstd: bool = True):
+        """(cells (n, 3) int32, counts int32, offset float32[3], ranges int32[3], hilbert)."""
+        cp, kp = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)()
+        n = C.c_uint64()
+        of = np.zeros(3, np.float32)
+        rg = np.zeros(3, np.int32)
+        hil = C.c_int()
+        N.check(N.decompress_to_cells(self.handle, data, len(data), int(is_zstd), C.byref(cp), C.byref(kp), C.byref(n),
+                                      of.ctypes.data_as(C.c_void_p), rg.ctypes.data_as(C.c_void_p), C.byref(hil)))
+        try:
+            cells = np.ctypeslib.as_array(cp, shape=(3 * n.value,)).copy().reshape(-1, 3) if n.value else \
+                np.zeros((0, 3), np.int32)
+            counts = np.ctypeslib.as_array(kp, shape=(n.value,)).copy() if n.value else np.zeros(0, np.int32)
+        finally:
+            N.free(C.cast(cp, C.c_void_p))
+            N.free(C.cast(kp, C.c_void_p))
+        return cells, counts, of, rg, bool(hil.value)
+
+    def expand_cells(self, cells, counts, offset, quantizer: int, l2: float) -> np.ndarray:
+        """expand_cells_to_points: points (sum(counts), 3) float32."""
+        cl = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        ct = np.ascontiguousarray(counts, dtype=np.int32)
+        of = np.ascontiguousarray(offset, dtype=np.float32)
+        out = C.POINTER(C.c_float)()
+        n = C.c_uint64()
+        N.check(N.expand_cells(self.handle, cl.ctypes.data_as(C.c_void_p), ct.ctypes.data_as(C.c_void_p), cl.shape[0],
+                               int(quantizer), float(l2), of.ctypes.data_as(C.c_void_p), C.byref(out), C.byref(n)))
+        try:
+            return np.ctypeslib.as_array(out, shape=(3 * n.value,)).copy().reshape(-1, 3) if n.value else \
+                np.zeros((0, 3), np.float32)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+
     def decompress_device(self, dev_ptr: int, length: int, quantizer: int, l2: float, rle: bool):
         """Device container -> (device pointer to 3*n floats owned by the context, n)."""
         p = C.c_void_p()

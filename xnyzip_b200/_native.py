@@ -120,6 +120,14 @@ mlp_adam = _proto("xnyz_mlp_adam", [_p, _p, _p, _p, C.c_float, C.c_int, _p])
 batch_roundtrip_device = _proto("xnyz_batch_roundtrip_device", [_p, C.c_uint64, _p, _p, _p, _p, _p, _p])
 batch_autotune = _proto("xnyz_batch_autotune", [_p, C.c_uint64, _p, _p, _p, _p])
 
+encode_cells = _proto("xnyz_encode_cells", [_p, _p, _p, C.c_uint64, C.c_int, _p, _p, C.c_int, C.c_int, _u8pp,
+                                            C.POINTER(C.c_uint64)])
+decompress_to_cells = _proto("xnyz_decompress_to_cells", [_p, _p, C.c_uint64, C.c_int, C.POINTER(C.POINTER(C.c_int32)),
+                                                          C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_uint64), _p,
+                                                          _p, C.POINTER(C.c_int)])
+expand_cells = _proto("xnyz_expand_cells", [_p, _p, _p, C.c_uint64, C.c_int, C.c_float, _p,
+                                            C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_uint64)])
+
 BLOCKS_OFF, BLOCKS_EXHAUSTIVE, BLOCKS_LEARNED, BLOCKS_GLOBAL = 0, 1, 2, 3
 
 # Every symbol include/xnyz.h declares (checked by the tests).
@@ -132,7 +140,8 @@ EXPORTED = [
     "xnyz_set_block_mode", "xnyz_set_model", "xnyz_model_param_count", "xnyz_last_block_info",
     "xnyz_batch_set_block_mode", "xnyz_stage_repos", "xnyz_block_features", "xnyz_block_search", "xnyz_block_cost",
     "xnyz_mlp_forward", "xnyz_mlp_gather_floats", "xnyz_mlp_train_batch", "xnyz_mlp_adam",
-    "xnyz_batch_roundtrip_device", "xnyz_batch_autotune",
+    "xnyz_batch_roundtrip_device", "xnyz_batch_autotune", "xnyz_encode_cells", "xnyz_decompress_to_cells",
+    "xnyz_expand_cells",
 ]
 
 

@@ -567,8 +567,18 @@ xnyz_status select_block_params(xnyz_ctx* c, const CPlan& cp, uint64_t U, uint64
     return XNYZ_OK;
 }
 
+// Cell-table input of encode_cells_with_counts (composer/block_compressor_rle.hpp:341-470):
+// device cells (int32 xyz) and counts, the global ranges and offset.  Block mode, -rle
+// container, one unit per cell, counts carried in the cells' container order.
+struct CellInput {
+    const int32_t* cells;
+    const int32_t* counts;
+    int32_t range[3];
+    float offset[3];
+};
+
 xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& prm, bool want_order,
-                          size_t arena_reserved, CompressOut& R) {
+                          size_t arena_reserved, CompressOut& R, const CellInput* cin = nullptr) {
     if (prm.quantizer != XNYZ_QUANT_CUBE && prm.quantizer != XNYZ_QUANT_TO)
         return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
     if (!(prm.l2_bound > 0.0f) || !std::isfinite(prm.l2_bound))
@@ -593,26 +603,49 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         CUDA_TRY(cudaMemcpyAsync(&c->d_small->stats, &c->h_small->stats, sizeof(PointStats), cudaMemcpyHostToDevice, st));
         TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
     }
-    {
-        Prof pr(c, "bbox", 1, 12.0 * n);
-        launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
-    }
-    {
-        Prof pr(c, "quantize_range", 1, 12.0 * n);
-        launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+    if (cin) {
+        for (int a = 0; a < 3; ++a) c->h_small->stats.max_cell[a] = INT32_MIN;
+        CUDA_TRY(cudaMemcpyAsync(&c->d_small->stats, &c->h_small->stats, sizeof(PointStats), cudaMemcpyHostToDevice, st));
+        launch_cells_stats(cin->cells, n, SMALL_FIELD(c, stats), st);
+    } else {
+        {
+            Prof pr(c, "bbox", 1, 12.0 * n);
+            launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
+        }
+        {
+            Prof pr(c, "quantize_range", 1, 12.0 * n);
+            launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+        }
     }
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, stats), sizeof(PointStats)));
-    const PointStats S = c->h_small->stats;
+    PointStats S = c->h_small->stats;
     hp1.end();
     HostPhase hp2(c, "c2_keys_sort_units");
-    if (S.nonfinite) return fail(XNYZ_ERR_UNSUPPORTED, "input contains NaN or infinite coordinates");
-    if (S.min_cell[0] < 0 || S.min_cell[1] < 0 || S.min_cell[2] < -1)
-        return fail(XNYZ_ERR_UNSUPPORTED, "lattice index outside the int range (coordinates too large for the bound)");
+    if (cin) {
+        // the reference indexes super-blocks from the given (global) ranges; cells outside
+        // them, or below zero other than the z = -1 cells of the truncated octahedron, would
+        // wrap its size_t arithmetic
+        for (int a = 0; a < 3; ++a)
+            if (S.max_cell[a] > cin->range[a] || cin->range[a] < 0)
+                return fail(XNYZ_ERR_UNSUPPORTED, "cells outside the given ranges");
+        if (S.min_cell[0] < 0 || S.min_cell[1] < 0 || S.min_cell[2] < -1)
+            return fail(XNYZ_ERR_UNSUPPORTED, "negative cell coordinates");
+        for (int a = 0; a < 3; ++a) {
+            S.max_cell[a] = cin->range[a];
+            S.offset[a] = cin->offset[a];
+        }
+        S.mse_max_bits = 0;
+        S.mse_sum = 0.0;
+    } else {
+        if (S.nonfinite) return fail(XNYZ_ERR_UNSUPPORTED, "input contains NaN or infinite coordinates");
+        if (S.min_cell[0] < 0 || S.min_cell[1] < 0 || S.min_cell[2] < -1)
+            return fail(XNYZ_ERR_UNSUPPORTED, "lattice index outside the int range (coordinates too large for the bound)");
+    }
     const int rx = S.max_cell[0], ry = S.max_cell[1], rz = S.max_cell[2];
     const bool defects = S.min_cell[2] < 0;  // truncated-octahedron cells at z = -1
     const int max_range = std::max({rx, ry, rz});
-    const bool direct = max_range < prm.direct_threshold;
+    const bool direct = !cin && max_range < prm.direct_threshold;  // cell tables: always block mode
 
     // ---- 2. key layout ----
     BlockKeyParams bkp{};
@@ -681,7 +714,10 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     CUDA_TRY(cudaMemcpyAsync(c->d_small->hil_inv, hm.inv.data(), 256, cudaMemcpyHostToDevice, st));
     {
         Prof pr(c, "keys", 1, 20.0 * n + (want_order ? 4.0 * n : 0.0));
-        if (direct)
+        if (cin)
+            launch_keys_cells(cin->cells, n, bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0], passes,
+                              c->d_small->sort_hist, st);
+        else if (direct)
             launch_keys_direct(d_xyz, n, q, SMALL_FIELD(c, stats), dkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
                                passes, c->d_small->sort_hist, st);
         else
@@ -720,8 +756,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
             launch_units_direct(sorted, n, rle, dkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
                                 SMALL_FIELD(c, err), st);
         else
-            launch_units_block(sorted, n, rle, bkp, uo, lb_state(c, lb_units), SMALL_FIELD(c, tile_counters[10]),
-                               SMALL_FIELD(c, err), st);
+            launch_units_block(sorted, n, cin ? 0 : rle, bkp, uo, lb_state(c, lb_units),
+                               SMALL_FIELD(c, tile_counters[10]), SMALL_FIELD(c, err), st);
     }
     CUDA_TRY(cudaGetLastError());
     TRY(fetch_small(c, offsetof(Small, counters), sizeof(unsigned long long) * 8));
@@ -739,7 +775,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         CountStats cs{c->d_small->cnt_hist, c->d_small->cnt_first, at<uint32_t>(c, o_over_v), at<uint32_t>(c, o_over_u),
                       SMALL_FIELD(c, over_n)};
         Prof pr(c, "count_stats", 1, 8.0 * U);
-        launch_count_stats(uo.unit_pos, U, n, at<int32_t>(c, o_counts), cs, st);
+        if (cin) launch_gather_i32(cin->counts, R.d_order, U, at<int32_t>(c, o_counts), st);  // container order
+        launch_count_stats(cin ? nullptr : uo.unit_pos, U, n, at<int32_t>(c, o_counts), cs, st);
     }
     if (!direct) {
         TRY(memset_small(c, offsetof(Small, max2), sizeof(unsigned long long) * 2, 0));
@@ -1007,8 +1044,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
 
 // Runs compress_core, growing the arena and retrying once when the encoders need more.
 xnyz_status compress_run(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& p, bool want_order,
-                         size_t reserved, CompressOut& R) {
-    xnyz_status s = compress_core(c, d_xyz, n, p, want_order, reserved, R);
+                         size_t reserved, CompressOut& R, const CellInput* cin = nullptr) {
+    xnyz_status s = compress_core(c, d_xyz, n, p, want_order, reserved, R, cin);
     if (s == XNYZ_ERR_OOM && g_last_error.rfind("__grow__:", 0) == 0) {
         const size_t need = std::stoull(g_last_error.substr(9));
         // Input points may live in the arena's reserved prefix: keep them.
@@ -1028,7 +1065,7 @@ xnyz_status compress_run(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz
             TRY(ensure_arena(c, need));
         }
         R = CompressOut{};
-        s = compress_core(c, d_xyz, n, p, want_order, reserved, R);
+        s = compress_core(c, d_xyz, n, p, want_order, reserved, R, cin);
     }
     return s;
 }
@@ -1184,8 +1221,12 @@ struct DecodeJob {
     uint64_t fill_value = 0;
 };
 
+// cells_out: decompress_to_cells (block_decompressor_rle.hpp:230-335): *d_out receives the
+// units' lattice cells (int32 xyz, container order, not expanded) and *cells_out the decoded
+// counts; otherwise *d_out receives the points.
 xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, const Header& h, int quantizer,
-                            float l2, bool rle, size_t reserved, float** d_out, uint64_t* n_out) {
+                            float l2, bool rle, size_t reserved, float** d_out, uint64_t* n_out,
+                            int32_t** cells_out = nullptr) {
     cudaStream_t st = c->stream;
     const QuantParams q = make_quant(quantizer, l2);
     const uint64_t U = h.units;
@@ -1455,7 +1496,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     if (!h.direct && NB && c->h_small->count_total != U)
         return fail(XNYZ_ERR_BAD_STREAM, "block counts do not add up to the point count");
     if (!h.direct && NB == 0 && U) return fail(XNYZ_ERR_BAD_STREAM, "no blocks");
-    const uint64_t nout = rle ? c->h_small->totals[0] : U;
+    const uint64_t nout = (rle && !cells_out) ? c->h_small->totals[0] : U;
     hd3.end();
     HostPhase hd4(c, "d4_recover");
 
@@ -1475,7 +1516,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     rp.ny = static_cast<uint64_t>(static_cast<int64_t>(h.ry)) / 128 + 1;
     rp.hilbert = h.hilbert;
     rp.hstart_inv = hm.inv_block_start;
-    rp.rle = rle;
+    rp.rle = rle && !cells_out;
+    rp.cells = cells_out != nullptr;
     rp.direct = h.direct;
     {
         int mr = std::max({h.rx, h.ry, h.rz}), bits = 0;
@@ -1507,14 +1549,15 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(check_device_errors(c));
     *d_out = out;
     *n_out = nout;
+    if (cells_out) *cells_out = at<int32_t>(c, o_counts);
     return XNYZ_OK;
 }
 
 xnyz_status decompress_run(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, const Header& h, int quantizer, float l2,
-                           bool rle, size_t reserved, float** d_out, uint64_t* n_out) {
+                           bool rle, size_t reserved, float** d_out, uint64_t* n_out, int32_t** cells_out = nullptr) {
     // The container may live in the arena's reserved prefix; growing keeps that prefix.
     for (int attempt = 0; attempt < 3; ++attempt) {
-        xnyz_status s = decompress_core(c, d_cont, len, h, quantizer, l2, rle, reserved, d_out, n_out);
+        xnyz_status s = decompress_core(c, d_cont, len, h, quantizer, l2, rle, reserved, d_out, n_out, cells_out);
         if (!(s == XNYZ_ERR_OOM && g_last_error.rfind("__grow__:", 0) == 0)) return s;
         const size_t need = std::stoull(g_last_error.substr(9));
         if (reserved) {
@@ -1866,6 +1909,168 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
     CUDA_TRY(cudaStreamSynchronize(st));
     *dev_xyz = d_out;
     *n = nout;
+    return XNYZ_OK;
+}
+
+// ---- distributed-RLE cell tables ------------------------------------------------------------
+xnyz_status xnyz_encode_cells(xnyz_ctx* c, const int32_t* cells, const int32_t* counts, uint64_t n,
+                              int cells_is_device, const int32_t* ranges, const float* offset, int hilbert,
+                              int use_zstd, uint8_t** out, uint64_t* out_len) {
+    clear_stale_cuda_error();
+    if (!c || !cells || !counts || !ranges || !offset || !out || !out_len)
+        return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (n == 0) return fail(XNYZ_ERR_INVALID_ARG, "no cells");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (use_zstd) {
+        std::string e;
+        if (!zstd_available(e)) return fail(XNYZ_ERR_ZSTD, e);
+    }
+    cudaStream_t st = c->stream;
+    // host tables are staged in a buffer of their own (the workspace may move while it grows)
+    int32_t* tmp = nullptr;
+    struct Free {
+        int32_t*& p;
+        ~Free() {
+            if (p) cudaFree(p);
+        }
+    } guard{tmp};
+    CellInput ci{};
+    if (cells_is_device) {
+        ci.cells = cells;
+        ci.counts = counts;
+    } else {
+        CUDA_TRY(cudaMalloc(&tmp, 16 * n));
+        CUDA_TRY(cudaMemcpyAsync(tmp, cells, 12 * n, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(tmp + 3 * n, counts, 4 * n, cudaMemcpyHostToDevice, st));
+        ci.cells = tmp;
+        ci.counts = tmp + 3 * n;
+    }
+    for (int a = 0; a < 3; ++a) {
+        ci.range[a] = ranges[a];
+        ci.offset[a] = offset[a];
+    }
+    const xnyz_params p{XNYZ_QUANT_TO, 1.0f, hilbert ? 1 : 0, 1, 0};
+    const int mode = c->block_mode;
+    c->block_mode = XNYZ_BLOCKS_OFF;  // the reference's container
+    CompressOut R;
+    xnyz_status s = ensure_arena(c, make_cplan(n, true, 0, false).total + encoder_reserve(n));
+    if (s == XNYZ_OK) s = compress_run(c, nullptr, n, p, true, 0, R, &ci);
+    c->block_mode = mode;
+    if (s != XNYZ_OK) return s;
+    const size_t clen = R.cont.size;
+    TRY(ensure_host_stage(c, clen));
+    CUDA_TRY(R.cont.to_host(c->h_stage, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    size_t cap = use_zstd ? zstd_bound(clen) : clen;
+    uint8_t* buf = static_cast<uint8_t*>(std::malloc(cap ? cap : 1));
+    if (!buf) return fail(XNYZ_ERR_OOM, "host allocation");
+    if (use_zstd) {
+        std::string e;
+        size_t w = 0;
+        if (!zstd_compress_into(c->h_stage, clen, 3, buf, cap, w, e)) {
+            std::free(buf);
+            return fail(XNYZ_ERR_ZSTD, e);
+        }
+        cap = w;
+    } else {
+        std::memcpy(buf, c->h_stage, clen);
+    }
+    *out = buf;
+    *out_len = cap;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_decompress_to_cells(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int32_t** cells,
+                                     int32_t** counts, uint64_t* n, float* offset, int32_t* ranges, int* hilbert) {
+    clear_stale_cuda_error();
+    if (!c || !in || !cells || !counts || !n || !offset || !ranges || !hilbert)
+        return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const uint8_t* raw = in;
+    uint64_t len = in_len;
+    std::string e;
+    if (is_zstd) {
+        uint64_t fs = 0;
+        if (!zstd_content_size(in, in_len, fs, e)) return fail(XNYZ_ERR_ZSTD, e);
+        TRY(ensure_host_stage(c, fs + 64));
+        if (!zstd_decompress(in, in_len, c->h_stage, fs, e)) return fail(XNYZ_ERR_ZSTD, e);
+        raw = c->h_stage;
+        len = fs;
+    }
+    Header h;
+    TRY(parse_header([&](uint64_t off, uint64_t bytes, void* dst) { std::memcpy(dst, raw + off, bytes); return true; },
+                     len, true, h));
+    if (h.direct) return fail(XNYZ_ERR_BAD_STREAM, "decompress_to_cells: a direct-mode container (cell tables use block mode)");
+    if (h.ext) return fail(XNYZ_ERR_UNSUPPORTED, "decompress_to_cells: an extended container");
+    const size_t reserved = align_up(len + 64);
+    TRY(ensure_arena(c, reserved));
+    CUDA_TRY(cudaMemcpyAsync(c->arena.base, raw, len, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(c->arena.base + len, 0, 64, st));
+    float* d_cells = nullptr;
+    int32_t* d_counts = nullptr;
+    uint64_t nu = 0;
+    TRY(decompress_run(c, reinterpret_cast<const uint8_t*>(c->arena.base), len, h, XNYZ_QUANT_TO, 1.0f, true, reserved,
+                       &d_cells, &nu, &d_counts));
+    int32_t* hc = static_cast<int32_t*>(std::malloc(12 * nu + 4));
+    int32_t* hk = static_cast<int32_t*>(std::malloc(4 * nu + 4));
+    if (!hc || !hk) {
+        std::free(hc);
+        std::free(hk);
+        return fail(XNYZ_ERR_OOM, "host allocation");
+    }
+    if (nu) {
+        CUDA_TRY(cudaMemcpyAsync(hc, d_cells, 12 * nu, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(hk, d_counts, 4 * nu, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *cells = hc;
+    *counts = hk;
+    *n = nu;
+    for (int a = 0; a < 3; ++a) offset[a] = h.off[a];
+    ranges[0] = h.rx;
+    ranges[1] = h.ry;
+    ranges[2] = h.rz;
+    *hilbert = h.hilbert ? 1 : 0;
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_expand_cells(xnyz_ctx* c, const int32_t* cells, const int32_t* counts, uint64_t n, int quantizer,
+                              float l2_bound, const float* offset, float** xyz, uint64_t* n_points) {
+    clear_stale_cuda_error();
+    if (!c || (n && (!cells || !counts)) || !offset || !xyz || !n_points)
+        return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; ++i) total += counts[i] > 0 ? static_cast<uint64_t>(counts[i]) : 0;
+    Plan pl;
+    const size_t o_cells = pl.add(12 * n + 16), o_counts = pl.add(4 * n + 16), o_off = pl.add(16),
+                 o_out = pl.add(12 * total + 16);
+    const LB lb = plan_lb(pl, cdiv(std::max<uint64_t>(n, 1), 4096), 1);
+    TRY(ensure_arena(c, pl.total));
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(at<int32_t>(c, o_cells), cells, 12 * n, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(at<int32_t>(c, o_counts), counts, 4 * n, cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(at<float>(c, o_off), offset, 12, cudaMemcpyHostToDevice, st));
+    TRY(lb_clear(c, lb, 1));
+    TRY(memset_small(c, offsetof(Small, err), sizeof(uint32_t), 0));
+    TRY(memset_small(c, offsetof(Small, tile_counters), sizeof(uint32_t) * 64, 0));
+    TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
+    launch_expand_cells(at<int32_t>(c, o_cells), at<int32_t>(c, o_counts), n, make_quant(quantizer, l2_bound),
+                        at<float>(c, o_off), lb_state(c, lb), SMALL_FIELD(c, tile_counters[0]), at<float>(c, o_out),
+                        total, SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), st);
+    CUDA_TRY(cudaGetLastError());
+    TRY(check_device_errors(c));
+    float* host = static_cast<float*>(std::malloc(12 * total + 4));
+    if (!host) return fail(XNYZ_ERR_OOM, "host allocation");
+    if (total) CUDA_TRY(cudaMemcpyAsync(host, at<float>(c, o_out), 12 * total, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *xyz = host;
+    *n_points = total;
     return XNYZ_OK;
 }
 

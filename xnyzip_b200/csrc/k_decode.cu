@@ -470,6 +470,14 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
             cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gather3(m >> 1));
             cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gather3(m >> 2));
         }
+        if (a.rp.cells) {
+            i32* co = reinterpret_cast<i32*>(a.out);
+            co[3 * opos] = cx;
+            co[3 * opos + 1] = cy;
+            co[3 * opos + 2] = cz;
+            ++opos;
+            continue;
+        }
         float x, y, z;
         recover(q, cx, cy, cz, a.rp.off[0], a.rp.off[1], a.rp.off[2], x, y, z);
         const u64 c = rle ? (u64)max(a.counts[base + e], 0) : 1ull;

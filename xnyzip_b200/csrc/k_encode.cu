@@ -209,9 +209,13 @@ __global__ void __launch_bounds__(kThreads) count_stats_kernel(const u32* __rest
         const bool ok = u < units;
         u32 c = 0;
         if (ok) {
-            const u64 nxt = (u + 1 < units) ? (u64)unit_pos[u + 1] : n;
-            c = (u32)(nxt - unit_pos[u]);
-            counts[u] = (i32)c;
+            if (unit_pos) {
+                const u64 nxt = (u + 1 < units) ? (u64)unit_pos[u + 1] : n;
+                c = (u32)(nxt - unit_pos[u]);
+                counts[u] = (i32)c;
+            } else {  // counts given (cell tables)
+                c = (u32)counts[u];
+            }
         }
         const bool dense = ok && c < (u32)kCountDense;
         hist_add(sh, sf, dense, c, (u32)u);

@@ -223,6 +223,106 @@ __global__ void __launch_bounds__(kThreads) keys_block_kernel(const float* __res
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
+// Cell tables (encode_cells_with_counts, composer/block_compressor_rle.hpp:341-470): block
+// keys straight from int32 lattice cells, and the per-axis minima / maxima of the cells.
+__global__ void __launch_bounds__(kThreads) keys_cells_kernel(const i32* __restrict__ cells, u64 n, BlockKeyParams kp,
+                                                              const u8* __restrict__ htab_g,
+                                                              unsigned long long* __restrict__ keys,
+                                                              u32* __restrict__ payload, int passes, u32* hist) {
+    __shared__ u8 htab[256];
+    __shared__ u32 sh[8 * 256];
+    stage_hilbert_table(htab_g, htab);
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    DigitHist dh{sh, passes};
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const u64 k = block_key(__ldg(cells + 3 * i), __ldg(cells + 3 * i + 1), __ldg(cells + 3 * i + 2), kp, htab);
+        keys[i] = k;
+        if (payload) payload[i] = (u32)i;
+        if (passes) dh.add(k);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+__global__ void __launch_bounds__(kThreads) cells_stats_kernel(const i32* __restrict__ cells, u64 n,
+                                                               PointStats* stats) {
+    i32 lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride)
+        for (int a = 0; a < 3; ++a) {
+            const i32 v = __ldg(cells + 3 * i + a);
+            lo[a] = min(lo[a], v);
+            hi[a] = max(hi[a], v);
+        }
+    for (int a = 0; a < 3; ++a) {
+        for (int d = 16; d > 0; d >>= 1) {
+            lo[a] = min(lo[a], __shfl_xor_sync(kFullMask, lo[a], d));
+            hi[a] = max(hi[a], __shfl_xor_sync(kFullMask, hi[a], d));
+        }
+        if (lane_id() == 0) {
+            atomicMin(&stats->min_cell[a], lo[a]);
+            atomicMax(&stats->max_cell[a], hi[a]);
+        }
+    }
+}
+
+__global__ void gather_i32_kernel(const i32* __restrict__ src, const u32* __restrict__ idx, u64 n,
+                                  i32* __restrict__ dst) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+// expand_cells_to_points (composer/block_decompressor_rle.hpp:339-358): every cell repeated
+// counts[i] times, recovered and unshifted; output positions by a chained scan of the counts.
+__global__ void __launch_bounds__(kThreads) expand_cells_kernel(const i32* __restrict__ cells,
+                                                                const i32* __restrict__ counts, u64 n, QuantParams q,
+                                                                const float* __restrict__ off3, LookBackState lb,
+                                                                u32* tile_counter, float* __restrict__ out, u64 cap,
+                                                                unsigned long long* total, u32* err) {
+    constexpr int kItems = 16, kTile = kThreads * kItems;
+    __shared__ u64 scratch[16];
+    __shared__ u32 slot;
+    __shared__ u64 sbase;
+    const u32 tile = claim_tile(tile_counter, &slot);
+    const u64 base = (u64)tile * kTile + (u64)threadIdx.x * kItems;
+    u64 s = 0;
+    for (int i = 0; i < kItems; ++i)
+        if (base + i < n) s += (u64)max(__ldg(counts + base + i), 0);
+    u64 tot;
+    const u64 ex = block_exclusive<kThreads>(s, 0ull, AddOp{}, scratch, tot);
+    if (threadIdx.x < 32) {
+        LookBack64 l{lb.flag, lb.agg, lb.inc};
+        const u64 r = warp_lookback_add(l, tile, tot, err);
+        if (threadIdx.x == 0) {
+            sbase = r;
+            if (tile == gridDim.x - 1) *total = r + tot;
+        }
+    }
+    __syncthreads();
+    u64 pos = sbase + ex;
+    const float ox = off3[0], oy = off3[1], oz = off3[2];
+    for (int i = 0; i < kItems; ++i) {
+        const u64 j = base + i;
+        if (j >= n) break;
+        const u64 c = (u64)max(__ldg(counts + j), 0);
+        if (pos + c > cap) {
+            atomicOr(err, kErrOverflow);
+            break;
+        }
+        float x, y, z;
+        recover(q, __ldg(cells + 3 * j), __ldg(cells + 3 * j + 1), __ldg(cells + 3 * j + 2), ox, oy, oz, x, y, z);
+        for (u64 r = 0; r < c; ++r) {
+            out[3 * (pos + r)] = x;
+            out[3 * (pos + r) + 1] = y;
+            out[3 * (pos + r) + 2] = z;
+        }
+        pos += c;
+    }
+}
+
 // Direct mode: key = global Morton or Hilbert code (hilbert_bits levels); z == -1 cells keep
 // their transformed low levels under defect_flag.
 __global__ void __launch_bounds__(kThreads) keys_direct_kernel(const float* __restrict__ xyz, u64 n, QuantParams q,
@@ -323,6 +423,22 @@ void launch_keys_direct(const float* xyz, uint64_t n, QuantParams q, const Point
                         uint32_t* hist, cudaStream_t st) {
     keys_direct_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, kp, hilbert_tab, keys, payload, passes,
                                                          hist);
+}
+void launch_keys_cells(const int32_t* cells, uint64_t n, BlockKeyParams kp, const uint8_t* hilbert_tab,
+                       unsigned long long* keys, uint32_t* payload, int passes, uint32_t* hist, cudaStream_t st) {
+    keys_cells_kernel<<<grid_for(n), kThreads, 0, st>>>(cells, n, kp, hilbert_tab, keys, payload, passes, hist);
+}
+void launch_cells_stats(const int32_t* cells, uint64_t n, PointStats* stats, cudaStream_t st) {
+    cells_stats_kernel<<<grid_for(n), kThreads, 0, st>>>(cells, n, stats);
+}
+void launch_gather_i32(const int32_t* src, const uint32_t* idx, uint64_t n, int32_t* dst, cudaStream_t st) {
+    if (n) gather_i32_kernel<<<grid_for(n), kThreads, 0, st>>>(src, idx, n, dst);
+}
+void launch_expand_cells(const int32_t* cells, const int32_t* counts, uint64_t n, QuantParams q, const float* off3,
+                         LookBackState lb, uint32_t* tile_counter, float* out, uint64_t cap,
+                         unsigned long long* total, uint32_t* err, cudaStream_t st) {
+    const unsigned tiles = (unsigned)((n + kThreads * 16 - 1) / (kThreads * 16));
+    if (tiles) expand_cells_kernel<<<tiles, kThreads, 0, st>>>(cells, counts, n, q, off3, lb, tile_counter, out, cap, total, err);
 }
 void launch_quantize_cells(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, int32_t* cells,
                            cudaStream_t st) {

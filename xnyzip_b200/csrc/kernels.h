@@ -102,6 +102,16 @@ void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointS
 void launch_keys_direct(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, DirectKeyParams kp,
                         const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
                         uint32_t* hist, cudaStream_t st);
+// Cell tables: block keys from int32 cells; per-axis min / max of cells (stats->min_cell /
+// max_cell, initialised by the caller); dst[i] = src[idx[i]]; expansion + recover + unshift
+// (lb: flag, agg, inc of ceil(n / 4096) tiles; *total receives the point count).
+void launch_keys_cells(const int32_t* cells, uint64_t n, BlockKeyParams kp, const uint8_t* hilbert_tab,
+                       unsigned long long* keys, uint32_t* payload, int passes, uint32_t* hist, cudaStream_t st);
+void launch_cells_stats(const int32_t* cells, uint64_t n, PointStats* stats, cudaStream_t st);
+void launch_gather_i32(const int32_t* src, const uint32_t* idx, uint64_t n, int32_t* dst, cudaStream_t st);
+void launch_expand_cells(const int32_t* cells, const int32_t* counts, uint64_t n, QuantParams q, const float* off3,
+                         LookBackState lb, uint32_t* tile_counter, float* out, uint64_t cap,
+                         unsigned long long* total, uint32_t* err, cudaStream_t st);
 void launch_quantize_cells(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, int32_t* cells,
                            cudaStream_t st);
 void launch_recover_cells(const int32_t* cells, uint64_t n, QuantParams q, const float* offset3_dev, float* xyz,
@@ -123,6 +133,7 @@ void launch_units_block(const unsigned long long* keys, uint64_t n, int rle, Blo
                         LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st);
 void launch_units_direct(const unsigned long long* keys, uint64_t n, int rle, DirectKeyParams kp, UnitOutputs out,
                          LookBackState lb, uint32_t* tile_counter, uint32_t* err, cudaStream_t st);
+// unit_pos null: counts[] is the input (cell tables), else counts[] receives the run lengths.
 void launch_count_stats(const uint32_t* unit_pos, uint64_t units, uint64_t n, int32_t* counts, CountStats cs,
                         cudaStream_t st);
 // Block deltas (blk ids and block unit counts) and their maxima.
@@ -202,7 +213,8 @@ struct RecoverParams {
     unsigned int hstart_inv;  // inverse-Hilbert state after levels 20..6 of zero digits
     int rle;
     int direct;
-    int bits;  // direct mode hilbert_bits
+    int bits;   // direct mode hilbert_bits
+    int cells;  // write the units' int32 lattice cells instead of points (no expansion, no recover)
 };
 struct RecoverInputs {
     const uint8_t* rep_sym;
