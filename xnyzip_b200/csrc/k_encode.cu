@@ -47,6 +47,25 @@ __device__ __forceinline__ void hist_add(u32* hist, u32* first, bool valid, u32 
     }
 }
 
+// The same update with the groups of equal symbols found through a per-warp bit mask in
+// shared memory (one atomicOr per lane) instead of match.any, which serialises on the
+// address-divergence pipe.  `masks` is zero on entry and on return.
+__device__ __forceinline__ void hist_add_masked(u32* masks, u32* hist, u32* first, bool valid, u32 sym, u32 unit) {
+    const u32 lane = lane_id();
+    if (valid) atomicOr(&masks[sym], 1u << lane);
+    __syncwarp();
+    if (valid) {
+        const u32 peers = masks[sym];
+        if (lane == (u32)(__ffs(peers) - 1)) {
+            atomicAdd(&hist[sym], (u32)__popc(peers));
+            atomicMin(&first[sym], unit);
+        }
+    }
+    __syncwarp();
+    if (valid) masks[sym] = 0u;
+    __syncwarp();
+}
+
 template <bool DIRECT>
 __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__ keys, u64 n, int rle,
                                                          BlockKeyParams bkp, DirectKeyParams dkp, UnitOutputs out,
@@ -56,6 +75,7 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     __shared__ u32 slot;
     __shared__ u64 sbase[3];
     __shared__ u32 hrep[256], frep[256], hquad[16], fquad[16];
+    __shared__ u32 mrep[kThreads / 32][256], mquad[kThreads / 32][16];
     __shared__ u64 psum[kThreads / 32];
 
     const u32 tile = claim_tile(tile_counter, &slot);
@@ -74,6 +94,8 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
         hquad[tid] = 0;
         fquad[tid] = 0xffffffffu;
     }
+    for (int i = tid; i < (kThreads / 32) * 256; i += kThreads) (&mrep[0][0])[i] = 0u;
+    if (tid < (kThreads / 32) * 16) (&mquad[0][0])[tid] = 0u;
     __syncthreads();
 
     // Element e of the tile: flags (bit0 head, bit1 patch, bit2 new block, bits 8..15 quad
@@ -119,16 +141,23 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
         }
         return f;
     };
-    // Pass A: count heads, patches and new blocks of my 16 consecutive elements.
+    // Warp w owns elements [512 w, 512 w + 512) of the tile, taken 32 consecutive elements
+    // (one per lane) per round: staged keys are read without bank conflicts, and the
+    // outputs of a round land in consecutive units, so the stores coalesce.
+    const int w = tid >> 5;
+    const u32 lane = lane_id();
+    const u32 wfirst = (u32)w * (32u * kItems);
+    // Pass A: count heads, patches and new blocks of my 16 elements.
     u32 h = 0, p = 0, b = 0;
-    for (int i = 0; i < kItems; ++i) {
+    for (int r = 0; r < kItems; ++r) {
         u64 v, id;
-        const u32 f = classify((u32)tid * kItems + i, v, id);
+        const u32 f = classify(wfirst + (u32)r * 32u + lane, v, id);
         h += f & 1u;
         p += (f >> 1) & 1u;
         b += (f >> 2) & 1u;
     }
-    // Packed three-field exclusive scan: each field <= 4096 per tile, 21 bits apiece.
+    // Packed three-field exclusive scan: each field <= 4096 per tile, 21 bits apiece.  Lane
+    // 0's exclusive prefix is the count over the earlier warps' elements.
     const u64 mine = (u64)h | ((u64)p << 21) | ((u64)b << 42);
     u64 tot;
     const u64 ex = block_exclusive<kThreads>(mine, 0ull, AddOp{}, scratch, tot);
@@ -144,36 +173,44 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     }
     __syncthreads();
 
-    u64 uu = sbase[0] + (ex & ((1ull << 21) - 1));
-    u64 pp = sbase[1] + ((ex >> 21) & ((1ull << 21) - 1));
-    u64 bb = sbase[2] + ((ex >> 42) & ((1ull << 21) - 1));
+    const u64 wex = __shfl_sync(kFullMask, ex, 0);
+    u64 uu = sbase[0] + (wex & ((1ull << 21) - 1));
+    u64 pp = sbase[1] + ((wex >> 21) & ((1ull << 21) - 1));
+    u64 bb = sbase[2] + ((wex >> 42) & ((1ull << 21) - 1));
+    const u32 lt = lanemask_lt();
     u64 mysum = 0;
-    for (int i = 0; i < kItems; ++i) {
+    for (int r = 0; r < kItems; ++r) {
+        const u32 e = wfirst + (u32)r * 32u + lane;
         u64 vi, idi;
-        const u32 f = classify((u32)tid * kItems + i, vi, idi);
+        const u32 f = classify(e, vi, idi);
         const bool head = f & 1u;
-        const bool patch = (f >> 1) & 1u;
+        const bool patch = head && ((f >> 1) & 1u);
+        const bool nblk = head && ((f >> 2) & 1u);
+        const u32 hm = __ballot_sync(kFullMask, head), pm = __ballot_sync(kFullMask, patch),
+                  bm = __ballot_sync(kFullMask, nblk);
+        const u64 u = uu + __popc(hm & lt);
         const u32 sym = head ? (patch ? 0u : (u32)vi + 1u) : 0u;
         const u32 qsym = ((f >> 8) & 0xffu) + 1u;
         if (head) {
-            out.rep_sym[uu] = (u8)sym;
-            if (out.rep_val) out.rep_val[uu] = vi;
-            if (!DIRECT) out.quad_sym[uu] = (u8)qsym;
+            out.rep_sym[u] = (u8)sym;
+            if (out.rep_val) out.rep_val[u] = vi;
+            if (!DIRECT) out.quad_sym[u] = (u8)qsym;
             if (patch) {
-                out.patches[pp] = vi;
+                out.patches[pp + __popc(pm & lt)] = vi;
                 mysum += vi;
             }
-            if (!DIRECT && ((f >> 2) & 1u)) {
-                out.blk_id[bb] = idi;
-                out.blk_unit[bb] = (u32)uu;
+            if (!DIRECT && nblk) {
+                const u64 bi = bb + __popc(bm & lt);
+                out.blk_id[bi] = idi;
+                out.blk_unit[bi] = (u32)u;
             }
-            if (rle) out.unit_pos[uu] = (u32)(base + (u32)tid * kItems + i);
+            if (rle) out.unit_pos[u] = (u32)(base + e);
         }
-        hist_add(hrep, frep, head, sym, (u32)uu);
-        if (!DIRECT) hist_add(hquad, fquad, head, qsym, (u32)uu);
-        uu += head;
-        pp += head && patch;
-        bb += head && ((f >> 2) & 1u);
+        hist_add_masked(mrep[w], hrep, frep, head, sym, (u32)u);
+        if (!DIRECT) hist_add_masked(mquad[w], hquad, fquad, head, qsym, (u32)u);
+        uu += __popc(hm);
+        pp += __popc(pm);
+        bb += __popc(bm);
     }
     for (int d = 16; d > 0; d >>= 1) mysum += __shfl_xor_sync(kFullMask, mysum, d);
     if (lane_id() == 0) psum[tid >> 5] = mysum;

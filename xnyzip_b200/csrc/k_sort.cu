@@ -6,8 +6,10 @@
 // the key kernels order exactly as (id, reid) resp. (sfc, index) do, and only the digits
 // that can be non-zero are sorted.
 //
-// Per pass: each warp ranks its 512 keys with __match_any_sync (warp-private digit
-// counters), the block turns warp counts into tile-local digit offsets, one thread per
+// Per pass: each warp ranks its 512 keys against warp-private digit counters, finding the
+// lanes that share a digit through a per-warp bit mask in shared memory (one atomicOr per
+// lane: cheaper than match.any, which serialises on the address-divergence pipe), the
+// block turns warp counts into tile-local digit offsets, one thread per
 // digit resolves the tile's global base by look-back over the previous tiles' digit counts
 // (epoch-tagged 64-bit status words, so the status array is never cleared between passes),
 // keys are staged in shared memory in digit order and written out in coalesced runs.
@@ -59,8 +61,9 @@ __device__ u64 digit_lookback(u64* status, u32 tile, u32 d, u64 count, u32 epoch
     return acc;
 }
 
+// Keys only: 4 CTAs per SM (64 registers, 52 KB shared); with payload: 3.
 template <bool PAYLOAD>
-__global__ void __launch_bounds__(kThreads, 3) sort_pass_kernel(const u64* __restrict__ kin, u64* __restrict__ kout,
+__global__ void __launch_bounds__(kThreads, PAYLOAD ? 3 : 4) sort_pass_kernel(const u64* __restrict__ kin, u64* __restrict__ kout,
                                                              const u32* __restrict__ vin, u32* __restrict__ vout,
                                                              u64 n, int shift, const u32* __restrict__ offsets,
                                                              u64* status, u32 epoch, u32* tile_counter, u32* err) {
@@ -71,12 +74,16 @@ __global__ void __launch_bounds__(kThreads, 3) sort_pass_kernel(const u64* __res
     u32* dstart = whist + kWarps * kRadix;                                      // kRadix
     u32* scratch = dstart + kRadix;                                             // 16
     u32* slot = scratch + 16;                                                   // 1
-    u32* svals = slot + 16;                                                     // kTile (PAYLOAD)
+    u32* dmask = slot + 16;                                                     // kWarps * kRadix
+    u32* svals = dmask + kWarps * kRadix;                                       // kTile (PAYLOAD)
 
     const u32 tile = claim_tile(tile_counter, slot);
     const u64 base = (u64)tile * kTile;
     const int tid = threadIdx.x, w = tid >> 5, lane = lane_id();
-    for (int i = tid; i < kWarps * kRadix; i += kThreads) whist[i] = 0;
+    for (int i = tid; i < kWarps * kRadix; i += kThreads) {
+        whist[i] = 0;
+        dmask[i] = 0;
+    }
     __syncthreads();
 
     u64 k[kItems];
@@ -91,15 +98,23 @@ __global__ void __launch_bounds__(kThreads, 3) sort_pass_kernel(const u64* __res
         if (PAYLOAD) v[i] = ok ? vin[j] : 0u;
     }
     u32* wh = whist + w * kRadix;
+    u32* wm = dmask + w * kRadix;
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         const bool ok = wbase + (u64)i * 32 + lane < n;
         const u32 d = (u32)(k[i] >> shift) & 255u;
-        const u32 peers = __match_any_sync(kFullMask, ok ? d : (0x100u | (u32)lane));
-        u32 prev = 0;
-        if (ok) prev = wh[d];
+        if (ok) atomicOr(&wm[d], 1u << lane);
         __syncwarp();
-        if (ok && (u32)lane == (u32)(__ffs(peers) - 1)) wh[d] = prev + __popc(peers);
+        u32 peers = 0, prev = 0;
+        if (ok) {
+            peers = wm[d];
+            prev = wh[d];
+        }
+        __syncwarp();
+        if (ok && (u32)lane == (u32)(__ffs(peers) - 1)) {
+            wh[d] = prev + __popc(peers);
+            wm[d] = 0;
+        }
         __syncwarp();
         rank[i] = prev + __popc(peers & lanemask_lt());
     }
@@ -147,7 +162,8 @@ __global__ void __launch_bounds__(kThreads, 3) sort_pass_kernel(const u64* __res
 }
 
 constexpr size_t smem_bytes(bool payload) {
-    return kTile * 8 + kRadix * 8 + kWarps * kRadix * 4 + kRadix * 4 + 32 * 4 + (payload ? kTile * 4 : 0);
+    return kTile * 8 + kRadix * 8 + kWarps * kRadix * 4 + kRadix * 4 + 32 * 4 + kWarps * kRadix * 4 +
+           (payload ? kTile * 4 : 0);
 }
 
 __global__ void __launch_bounds__(kThreads) histogram_kernel(const u64* __restrict__ keys, u64 n, int passes,
