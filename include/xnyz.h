@@ -10,7 +10,10 @@
  *                       XnYZip::BlockCompressorRLE<float>::compress     composer/block_compressor_rle.hpp:34,38
  *   xnyz_decompress  <- XnYZip::BlockDecompressor<float>::decompress    composer/block_decompressor.hpp:27,31
  *                       XnYZip::BlockDecompressorRLE<float>::decompress composer/block_decompressor_rle.hpp:28,32
- *   quantizer codes  <- XnYZip::QUANTIZER_TYPE {CUBE, TRUNCATED_OCTAHEDRON} composer/utils.hpp:55-59
+ *   quantizer codes  <- XnYZip::QUANTIZER_TYPE {CUBE, TRUNCATED_OCTAHEDRON, ADAPTIVE} composer/utils.hpp:55-59
+ *                       (ADAPTIVE: AdaptiveQuantizer quantizer/adaptive_quantizer.hpp:16-97, its three
+ *                       steps in the container's params; the stage entry points and the cell tables
+ *                       take cube and truncated octahedron only)
  *   stage entry points (xnyz_stage_*) <- shift_points preprocessor/shifting.hpp:11,
  *       TruncatedOctahedronQuantizer/CubeQuantizer::quantize/recover quantizer/truncated_octahedron_quantizer.hpp, cube_quantizer.hpp,
  *       mve::mortonToHilbert3/hilbertToMorton3 quantizer/hilbert-curves-cpp/hilbert.hpp:8-9,
@@ -42,13 +45,13 @@ typedef enum xnyz_status {
 } xnyz_status;
 
 /* Quantizer codes (values follow XnYZip::QUANTIZER_TYPE). */
-enum { XNYZ_QUANT_CUBE = 0, XNYZ_QUANT_TO = 1 };
+enum { XNYZ_QUANT_CUBE = 0, XNYZ_QUANT_TO = 1, XNYZ_QUANT_ADAPTIVE = 2 };
 
 typedef struct xnyz_ctx xnyz_ctx;
 
 /* Per-call configuration, mirroring the reference constructors and CLI flags. */
 typedef struct xnyz_params {
-    int quantizer;        /* XNYZ_QUANT_CUBE or XNYZ_QUANT_TO ("cube" / "to") */
+    int quantizer;        /* XNYZ_QUANT_CUBE, XNYZ_QUANT_TO ("cube" / "to") or XNYZ_QUANT_ADAPTIVE */
     float l2_bound;       /* the L2 bound (CLI argv[3]) */
     int hilbert;          /* 1 = Hilbert curve ("-h"), 0 = Morton / z-order ("-z") */
     int rle;              /* 1 = "-rle" container, 0 = "-normal" */

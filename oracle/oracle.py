@@ -25,7 +25,7 @@ REF_CLI = os.path.join(HERE, "_ref", "xnyzip_ref")
 sys.path.insert(0, HERE)
 from find_zstd import find_zstd  # noqa: E402
 
-QUANT = {"cube": 0, "to": 1}
+QUANT = {"cube": 0, "to": 1, "adaptive": 2}
 
 _u8p = C.POINTER(C.c_uint8)
 _f32p = C.POINTER(C.c_float)

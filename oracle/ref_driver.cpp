@@ -28,6 +28,7 @@ namespace {
 using P3 = Eigen::RowVector3f;
 
 XnYZip::QUANTIZER_TYPE qtype(int q) {
+    if (q == 2) return XnYZip::QUANTIZER_TYPE::ADAPTIVE;
     return q == 1 ? XnYZip::QUANTIZER_TYPE::TRUNCATED_OCTAHEDRON : XnYZip::QUANTIZER_TYPE::CUBE;
 }
 

@@ -144,6 +144,42 @@ void recover_cube(const i32 c[3], const QConst& k, float out[3]) {
     for (int d = 0; d < 3; ++d) out[d] = (((static_cast<float>(c[d]) + 0.5f) * 2.0f) * k.s) / k.rsqrt;
 }
 
+// AdaptiveQuantizer (quantizer/adaptive_quantizer.hpp:16-97): per-axis steps from the
+// extent of the shifted points, a = R * (max_x - min_x) / norm with norm the extent's
+// length (R / sqrt(3) on every axis when norm is 0); the maxima start at the smallest
+// normal float and the minima at FLT_MAX, as there.  Cells are round(p / step) cast to int,
+// points idx * step.
+void adaptive_steps(const float* xyz, u64 n, const float off[3], float R, float step[3]) {
+    float mn[3], mx[3];
+    for (int k = 0; k < 3; ++k) {
+        mn[k] = std::numeric_limits<float>::max();
+        mx[k] = std::numeric_limits<float>::min();
+    }
+    for (u64 i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float p = xyz[3 * i + k] - off[k];
+            mn[k] = std::min(mn[k], p);
+            mx[k] = std::max(mx[k], p);
+        }
+    const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    const float norm = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (norm > 0) {
+        step[0] = R * dx / norm;
+        step[1] = R * dy / norm;
+        step[2] = R * dz / norm;
+    } else {
+        step[0] = step[1] = step[2] = R / std::sqrt(3.0f);
+    }
+}
+
+void quantize_adaptive(const float p[3], const float step[3], i32 out[3]) {
+    for (int k = 0; k < 3; ++k) out[k] = f2i(std::round(p[k] / step[k]));
+}
+
+void recover_adaptive(const i32 c[3], const float step[3], float out[3]) {
+    for (int k = 0; k < 3; ++k) out[k] = static_cast<float>(c[k]) * step[k];
+}
+
 // ------------------------------------------------------------------ Morton ------------
 // split_by_3 / morton_code / compact_by_3 (preprocessor/z_order_curve.hpp:14-47):
 // 21 bits per axis, x at bit 0, y at bit 1, z at bit 2.
@@ -289,14 +325,25 @@ void shift_offset(const float* xyz, u64 n, float off[3]) {
             if (xyz[3 * i + k] < off[k]) off[k] = xyz[3 * i + k];
 }
 
-void quantize_all(const float* xyz, u64 n, int quantizer, float l2, float off[3], std::vector<i32>& q) {
+// shift_points + quantize; `params` receives the quantizer's parameters (the adaptive
+// steps; none for TO and cube).
+void quantize_all(const float* xyz, u64 n, int quantizer, float l2, float off[3], std::vector<i32>& q,
+                  std::vector<float>* params = nullptr) {
     shift_offset(xyz, n, off);
     QConst c = make_const(quantizer, l2);
+    float step[3] = {0, 0, 0};
+    if (quantizer == 2) adaptive_steps(xyz, n, off, l2, step);
+    if (params) {
+        params->clear();
+        if (quantizer == 2) params->assign(step, step + 3);
+    }
     q.resize(3 * n);
     for (u64 i = 0; i < n; ++i) {
         float p[3] = {xyz[3 * i] - off[0], xyz[3 * i + 1] - off[1], xyz[3 * i + 2] - off[2]};
         if (quantizer == 1)
             quantize_to(p, c.div, &q[3 * i]);
+        else if (quantizer == 2)
+            quantize_adaptive(p, step, &q[3 * i]);
         else
             quantize_cube(p, c.div, &q[3 * i]);
     }
@@ -770,7 +817,8 @@ Bytes compress_container(const float* xyz, u64 n, int quantizer, float l2, bool 
                          std::vector<u64>* order) {
     float off[3];
     std::vector<i32> q;
-    quantize_all(xyz, n, quantizer, l2, off, q);
+    std::vector<float> params;
+    quantize_all(xyz, n, quantizer, l2, off, q, &params);
     std::vector<Cell> cells(n);
     for (u64 i = 0; i < n; ++i) cells[i] = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
 
@@ -803,7 +851,8 @@ Bytes compress_container(const float* xyz, u64 n, int quantizer, float l2, bool 
 
     Writer w;
     w.pod<u64>(m);
-    w.pod<u64>(0);  // params.size(): TO and cube have none
+    w.pod<u64>(params.size());  // TO and cube have none, adaptive its three steps
+    for (float v : params) w.pod<float>(v);
     int rx = 0, ry = 0, rz = 0;
     for (auto& c : cells) {
         rx = std::max(rx, c.x);
@@ -890,7 +939,9 @@ std::vector<float> decompress_container(const Bytes& buf, int quantizer, float l
     Reader r{buf.data(), buf.data() + buf.size()};
     u64 n = r.pod<u64>();
     u64 np = r.pod<u64>();
-    for (u64 i = 0; i < np; ++i) r.pod<float>();
+    std::vector<float> params;
+    for (u64 i = 0; i < np; ++i) params.push_back(r.pod<float>());
+    if (quantizer == 2 && !rle && np < 3) throw std::runtime_error("adaptive container without its three steps");
     i32 rx = r.pod<i32>(), ry = r.pod<i32>(), rz = r.pod<i32>();
     bool hil = r.pod<bool>(), direct = r.pod<bool>();
     std::vector<Cell> cells(n);
@@ -966,8 +1017,12 @@ std::vector<float> decompress_container(const Bytes& buf, int quantizer, float l
     for (size_t i = 0; i < full.size(); ++i) {
         i32 c[3] = {full[i].x, full[i].y, full[i].z};
         float p[3];
+        // BlockDecompressorRLE picks TO or else cube (block_decompressor_rle.hpp:189-196):
+        // adaptive -rle containers are recovered with the cube quantizer there.
         if (quantizer == 1)
             recover_to(c, k, p);
+        else if (quantizer == 2 && !rle)
+            recover_adaptive(c, params.data(), p);
         else
             recover_cube(c, k, p);
         for (int d = 0; d < 3; ++d) out[3 * i + d] = p[d] + off[d];

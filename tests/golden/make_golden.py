@@ -39,6 +39,16 @@ def cases():
     base = rng.uniform(0, 100, (150, 3)).astype(np.float32)
     yield "egcounts_to_h_rle", np.repeat(base, rng.integers(1, 90, 150), axis=0), "to", 0.01, 1, 1, 1024
     yield "single_point", np.array([[1.5, -2.0, 3.25]], np.float32), "to", 0.05, 0, 1, 1024
+    # AdaptiveQuantizer (quantizer/adaptive_quantizer.hpp): steps in the params, block and
+    # direct mode, a flat axis (extent = the smallest normal float), and -rle, whose decoder
+    # recovers the cells with the cube quantizer (block_decompressor_rle.hpp:189-196)
+    yield "terrain_adaptive_h_normal", S.terrain(1500, 29, extent=300.0, amplitude=3.0, wavelength=150.0), \
+        "adaptive", 0.05, 1, 0, 1024
+    yield "direct_adaptive_z_normal", rng.uniform(0, 3, (1500, 3)).astype(np.float32), "adaptive", 0.05, 0, 0, 1024
+    flat = rng.uniform(0, 200, (1500, 3)).astype(np.float32)
+    flat[:, 2] = 4.25
+    yield "flat_adaptive_h_normal", flat, "adaptive", 0.01, 1, 0, 1024
+    yield "uniform_adaptive_h_rle", S.uniform(1500, 30), "adaptive", 0.05, 1, 1, 1024
 
 
 def main():
@@ -55,7 +65,7 @@ def main():
             ref.quiet(False)
         names.append(name)
         out[f"{name}/points"] = x
-        out[f"{name}/params"] = np.array([0 if q == "cube" else 1, hil, rle, th], np.int64)
+        out[f"{name}/params"] = np.array([{"cube": 0, "to": 1, "adaptive": 2}[q], hil, rle, th], np.int64)
         out[f"{name}/l2"] = np.array([l2], np.float32)
         out[f"{name}/frame"] = np.frombuffer(frame, np.uint8)
         out[f"{name}/container"] = np.frombuffer(raw, np.uint8)

@@ -41,6 +41,9 @@ def test_cells_roundtrip_matches_reference(ctx, reference, hilbert):
         assert o2.tobytes() == ro.tobytes() and np.array_equal(r2, rr) and h2 == rh
         pts = ctx.expand_cells(c2, k2, o2, {"cube": 0, "to": 1}[q], l2)
         assert pts.tobytes() == quiet_call(reference, reference.expand_cells, rc, rk, ro, q, l2).tobytes(), name
+        # expand_cells_to_points has no adaptive branch: the cube quantizer recovers the cells
+        pts = ctx.expand_cells(c2, k2, o2, 2, l2)
+        assert pts.tobytes() == quiet_call(reference, reference.expand_cells, rc, rk, ro, "adaptive", l2).tobytes()
 
 
 def test_cells_reject_direct_and_out_of_range(ctx, xnyz):

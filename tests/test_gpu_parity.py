@@ -11,8 +11,7 @@ from conftest import small_inputs
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_fixtures.npz")
-Q = {0: 0, 1: 1}
-QN = {0: "cube", 1: "to"}
+QN = {0: "cube", 1: "to", 2: "adaptive"}
 
 
 def golden_names():
@@ -34,7 +33,7 @@ def test_gpu_matches_reference_fixture(ctx, name):
     assert dec.tobytes() == f[f"{name}/decoded"].tobytes()
 
 
-MODES = [(q, l2, hil, rle, th) for q in (0, 1) for l2 in (0.05, 0.5) for hil in (0, 1) for rle in (0, 1)
+MODES = [(q, l2, hil, rle, th) for q in (0, 1, 2) for l2 in (0.05, 0.5) for hil in (0, 1) for rle in (0, 1)
          for th in (1024, 0)]
 
 
@@ -94,3 +93,18 @@ def test_gpu_normal_order_is_a_sort_permutation(ctx, oracle):
     # equal cells may appear in any order; the cells in container order must agree
     oq = oracle.quantize(x, "to", 0.05)[1]
     assert np.array_equal(oq[order.astype(np.int64)], oq[oorder.astype(np.int64)])
+
+
+def test_gpu_adaptive_zero_step_refused(ctx, xnyz):
+    """A flat axis gets the step R * FLT_MIN / norm, which underflows to 0 when the cloud is
+    large against the bound; the reference then casts NaN cells to INT_MIN and emits a
+    container that does not decode to the input.  The GPU path refuses such clouds."""
+    rng = np.random.default_rng(3)
+    x = np.c_[rng.random((3000, 2)) * 1e6, np.full(3000, 7.5)].astype(np.float32)
+    with pytest.raises(xnyz.XnyzError) as e:
+        ctx.compress(x, 2, 0.001, 1, 0)
+    assert e.value.status == 6
+    # a bound large enough keeps the step positive: flat axis at cell 0, exact round trip on z
+    frame = ctx.compress(x, 2, 10.0, 1, 0)
+    dec = ctx.decompress(frame, 2, 10.0, 0)
+    assert np.all(dec[:, 2] == np.float32(7.5))

@@ -13,7 +13,7 @@ import pytest
 from conftest import quiet_call, small_inputs
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_fixtures.npz")
-Q = {0: "cube", 1: "to"}
+Q = {0: "cube", 1: "to", 2: "adaptive"}
 
 
 def golden_cases():
@@ -49,7 +49,7 @@ def test_oracle_config1_digest(oracle):
     assert hashlib.sha256(dec.tobytes()).digest() == f["config1/decoded_sha256"].tobytes()
 
 
-MODES = [(q, l2, hil, rle, th) for q in ("to", "cube") for l2 in (0.05, 0.5) for hil in (0, 1) for rle in (0, 1)
+MODES = [(q, l2, hil, rle, th) for q in ("to", "cube", "adaptive") for l2 in (0.05, 0.5) for hil in (0, 1) for rle in (0, 1)
          for th in (1024, 0)]
 
 

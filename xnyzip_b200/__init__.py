@@ -332,9 +332,7 @@ class _CompressorBase:
 
     def __init__(self, quantizer_type: QUANTIZER_TYPE, l2_bound: float, is_debugging: bool = False,
                  direct_threshold: int = 1024, context: Context | None = None):
-        if QUANTIZER_TYPE(quantizer_type) == QUANTIZER_TYPE.ADAPTIVE:
-            raise XnyzError(6, "the adaptive quantizer is not on the CLI path (main.cpp handles cube and to)")
-        self.quantizer = int(quantizer_type)
+        self.quantizer = int(QUANTIZER_TYPE(quantizer_type))
         self.l2_bound = float(np.float32(l2_bound))
         self.direct_threshold = int(direct_threshold)
         self.ctx = context
@@ -370,9 +368,7 @@ class _DecompressorBase:
 
     def __init__(self, quantizer_type: QUANTIZER_TYPE, l2_bound: float, is_debugging: bool = False,
                  context: Context | None = None):
-        if QUANTIZER_TYPE(quantizer_type) == QUANTIZER_TYPE.ADAPTIVE:
-            raise XnyzError(6, "the adaptive quantizer is not on the CLI path")
-        self.quantizer = int(quantizer_type)
+        self.quantizer = int(QUANTIZER_TYPE(quantizer_type))
         self.l2_bound = float(np.float32(l2_bound))
         self.ctx = context
 

@@ -281,7 +281,7 @@ xnyz_status check_device_errors(xnyz_ctx* c) {
 }
 
 QuantParams make_quant(int quantizer, float l2) {
-    QuantParams q;
+    QuantParams q{};
     q.quantizer = quantizer;
     const double k = quantizer == 1 ? 5.0 : 3.0;
     // 2 * l2 in float, divided by sqrt(k) in double, stored as float (the reference's
@@ -579,14 +579,18 @@ struct CellInput {
 
 xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xnyz_params& prm, bool want_order,
                           size_t arena_reserved, CompressOut& R, const CellInput* cin = nullptr) {
-    if (prm.quantizer != XNYZ_QUANT_CUBE && prm.quantizer != XNYZ_QUANT_TO)
-        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    if (prm.quantizer != XNYZ_QUANT_CUBE && prm.quantizer != XNYZ_QUANT_TO && prm.quantizer != XNYZ_QUANT_ADAPTIVE)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube), 1 (truncated octahedron) or 2 (adaptive)");
+    if (cin && prm.quantizer == XNYZ_QUANT_ADAPTIVE)
+        return fail(XNYZ_ERR_INVALID_ARG, "cell tables take the cube or truncated-octahedron quantizer");
     if (!(prm.l2_bound > 0.0f) || !std::isfinite(prm.l2_bound))
         return fail(XNYZ_ERR_INVALID_ARG, "l2_bound must be a positive finite float");
     if (n == 0) return fail(XNYZ_ERR_INVALID_ARG, "no points (the reference leaves the offset undefined for n = 0)");
     if (n >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 points");
     const bool rle = prm.rle != 0, hil = prm.hilbert != 0;
-    const QuantParams q = make_quant(prm.quantizer, prm.l2_bound);
+    const bool adaptive = prm.quantizer == XNYZ_QUANT_ADAPTIVE;
+    QuantParams q = make_quant(prm.quantizer, prm.l2_bound);
+    if (adaptive) q.step_dev = SMALL_FIELD(c, stats.step[0]);  // written by launch_adaptive_steps
     cudaStream_t st = c->stream;
 
     // ---- 1. bounding box + quantization sweep ----
@@ -612,6 +616,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
             Prof pr(c, "bbox", 1, 12.0 * n);
             launch_bbox(d_xyz, n, SMALL_FIELD(c, stats), st);
         }
+        if (adaptive) launch_adaptive_steps(d_xyz, prm.l2_bound, SMALL_FIELD(c, stats), st);
         {
             Prof pr(c, "quantize_range", 1, 12.0 * n);
             launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
@@ -973,7 +978,12 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     Container& K = R.cont;
     if (ext) K.pod<uint64_t>(kExtMagic);
     K.pod<uint64_t>(U);
-    K.pod<uint64_t>(0);  // params.size(): the cube and truncated-octahedron quantizers have none
+    if (adaptive) {  // params: the adaptive quantizer's three steps (block_compressor.hpp:63-66)
+        K.pod<uint64_t>(3);
+        for (int a = 0; a < 3; ++a) K.pod<float>(S.step[a]);
+    } else {
+        K.pod<uint64_t>(0);  // the cube and truncated-octahedron quantizers have none
+    }
     K.pod<int32_t>(rx);
     K.pod<int32_t>(ry);
     K.pod<int32_t>(rz);
@@ -1081,6 +1091,7 @@ struct Header {
     int32_t rx = 0, ry = 0, rz = 0;
     bool hilbert = false, direct = false;
     std::vector<StreamRef> streams;
+    std::vector<float> params;  // quantizer parameters (adaptive: the three steps)
     float off[3] = {0, 0, 0};
 };
 
@@ -1104,7 +1115,10 @@ xnyz_status parse_header(Read rd, uint64_t len, bool rle, Header& h) {
     }
     if (!get(&np, 8)) return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
     if (np > (len - p) / 4) return fail(XNYZ_ERR_BAD_STREAM, "bad parameter count");
-    p += 4 * np;  // quantizer parameters (none for cube / truncated octahedron)
+    h.params.assign(np < 3 ? np : 3, 0.0f);  // only the adaptive quantizer reads them (three)
+    if (!h.params.empty() && !get(h.params.data(), 4 * h.params.size()))
+        return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
+    p += 4 * (np - h.params.size());
     if (!get(&h.rx, 4) || !get(&h.ry, 4) || !get(&h.rz, 4) || !get(&hb, 1) || !get(&db, 1))
         return fail(XNYZ_ERR_BAD_STREAM, "truncated container header");
     h.hilbert = hb != 0;
@@ -1228,7 +1242,14 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                             float l2, bool rle, size_t reserved, float** d_out, uint64_t* n_out,
                             int32_t** cells_out = nullptr) {
     cudaStream_t st = c->stream;
-    const QuantParams q = make_quant(quantizer, l2);
+    // BlockDecompressorRLE picks the truncated octahedron or else the cube quantizer
+    // (block_decompressor_rle.hpp:189-196): adaptive -rle containers recover as cube cells.
+    const int qrec = (rle && quantizer == XNYZ_QUANT_ADAPTIVE) ? XNYZ_QUANT_CUBE : quantizer;
+    QuantParams q = make_quant(qrec, l2);
+    if (qrec == XNYZ_QUANT_ADAPTIVE) {
+        if (h.params.size() < 3) return fail(XNYZ_ERR_BAD_STREAM, "adaptive container without its three steps");
+        for (int a = 0; a < 3; ++a) q.step[a] = h.params[a];
+    }
     const uint64_t U = h.units;
     if (U >= (1ull << 31)) return fail(XNYZ_ERR_UNSUPPORTED, "more than 2^31 - 1 cells");
     const auto& hm = hilbert_machines();
@@ -1804,8 +1825,8 @@ namespace {
 xnyz_status decompress_host_input(xnyz_ctx* c, const uint8_t* in, uint64_t in_len, int is_zstd, int quantizer,
                                   float l2_bound, int rle, float** d_out, uint64_t* nout) {
     if (!c || !in) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
-    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
-        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO && quantizer != XNYZ_QUANT_ADAPTIVE)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube), 1 (truncated octahedron) or 2 (adaptive)");
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     const uint8_t* raw = in;
@@ -1878,8 +1899,8 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
                                    float l2_bound, int rle, const float** dev_xyz, uint64_t* n) {
     clear_stale_cuda_error();
     if (!c || !dev_container || !dev_xyz || !n) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
-    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
-        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO && quantizer != XNYZ_QUANT_ADAPTIVE)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube), 1 (truncated octahedron) or 2 (adaptive)");
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     // The kernels read up to 16 bytes past a stream's end; containers from
@@ -2040,8 +2061,11 @@ xnyz_status xnyz_expand_cells(xnyz_ctx* c, const int32_t* cells, const int32_t* 
     clear_stale_cuda_error();
     if (!c || (n && (!cells || !counts)) || !offset || !xyz || !n_points)
         return fail(XNYZ_ERR_INVALID_ARG, "null argument");
-    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
-        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube) or 1 (truncated octahedron)");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO && quantizer != XNYZ_QUANT_ADAPTIVE)
+        return fail(XNYZ_ERR_INVALID_ARG, "quantizer must be 0 (cube), 1 (truncated octahedron) or 2 (adaptive)");
+    // expand_cells_to_points recovers with the truncated octahedron or else the cube
+    // quantizer (block_decompressor_rle.hpp:350-356)
+    if (quantizer == XNYZ_QUANT_ADAPTIVE) quantizer = XNYZ_QUANT_CUBE;
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     uint64_t total = 0;
@@ -2178,6 +2202,8 @@ xnyz_status xnyz_stage_quantize(xnyz_ctx* c, const float* dev_xyz, uint64_t n, i
                                 float* offset3, int32_t* dev_cells) {
     clear_stale_cuda_error();
     if (!c || !dev_xyz || !offset3 || !dev_cells || n == 0) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "stage quantizer must be 0 (cube) or 1 (truncated octahedron)");
     CUDA_TRY(cudaSetDevice(c->device));
     const QuantParams q = make_quant(quantizer, l2_bound);
     PointStats init{};
@@ -2200,6 +2226,8 @@ xnyz_status xnyz_stage_recover(xnyz_ctx* c, const int32_t* dev_cells, uint64_t n
                                const float* offset3, float* dev_xyz) {
     clear_stale_cuda_error();
     if (!c || !dev_cells || !offset3 || !dev_xyz) return fail(XNYZ_ERR_INVALID_ARG, "bad argument");
+    if (quantizer != XNYZ_QUANT_CUBE && quantizer != XNYZ_QUANT_TO)
+        return fail(XNYZ_ERR_INVALID_ARG, "stage quantizer must be 0 (cube) or 1 (truncated octahedron)");
     CUDA_TRY(cudaSetDevice(c->device));
     for (int a = 0; a < 3; ++a) c->h_small->offset_in[a] = offset3[a];
     CUDA_TRY(cudaMemcpyAsync(c->d_small->offset_in, c->h_small->offset_in, 12, cudaMemcpyHostToDevice, c->stream));

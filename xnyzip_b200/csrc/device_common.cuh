@@ -304,16 +304,33 @@ __device__ __forceinline__ void quantize_cube(float px, float py, float pz, floa
     oz = f2i_x86(floorf(__fdiv_rn(pz, div)));
 }
 
+// Adaptive quantizer steps: from device memory while compressing, from the container's
+// parameters while decompressing.
+__device__ __forceinline__ float adaptive_step(const QuantParams& q, int a) {
+    return q.step_dev ? q.step_dev[a] : q.step[a];
+}
+
+// Adaptive quantizer: round(p / step) per axis, half away from zero, then the x86 cast
+// (quantizer/adaptive_quantizer.hpp:66-77).
+__device__ __forceinline__ void quantize_adaptive(const QuantParams& q, float px, float py, float pz, i32& ox,
+                                                  i32& oy, i32& oz) {
+    ox = f2i_x86(roundf(__fdiv_rn(px, adaptive_step(q, 0))));
+    oy = f2i_x86(roundf(__fdiv_rn(py, adaptive_step(q, 1))));
+    oz = f2i_x86(roundf(__fdiv_rn(pz, adaptive_step(q, 2))));
+}
+
 __device__ __forceinline__ void quantize(const QuantParams& q, float px, float py, float pz, i32& ox, i32& oy,
                                          i32& oz) {
     if (q.quantizer == 1)
         quantize_to(px, py, pz, q.div, ox, oy, oz);
+    else if (q.quantizer == 2)
+        quantize_adaptive(q, px, py, pz, ox, oy, oz);
     else
         quantize_cube(px, py, pz, q.div, ox, oy, oz);
 }
 
 // Recover + unshift (truncated_octahedron_quantizer.hpp:57-76, cube_quantizer.hpp:29-38,
-// shifting.hpp:39-50).
+// adaptive_quantizer.hpp:83-97: idx * step, shifting.hpp:39-50).
 __device__ __forceinline__ void recover(const QuantParams& q, i32 cx, i32 cy, i32 cz, float offx, float offy,
                                         float offz, float& x, float& y, float& z) {
     float fx, fy, fz;
@@ -329,6 +346,10 @@ __device__ __forceinline__ void recover(const QuantParams& q, i32 cx, i32 cy, i3
         fx = __fdiv_rn(__fmul_rn(__fmul_rn(__int2float_rn(nx), 2.0f), q.s), q.rdiv);
         fy = __fdiv_rn(__fmul_rn(__fmul_rn(__int2float_rn(ny), 2.0f), q.s), q.rdiv);
         fz = __fdiv_rn(__fmul_rn(__fmul_rn(__int2float_rn(cz), 2.0f), q.s), q.rdiv);
+    } else if (q.quantizer == 2) {
+        fx = __fmul_rn(__int2float_rn(cx), adaptive_step(q, 0));
+        fy = __fmul_rn(__int2float_rn(cy), adaptive_step(q, 1));
+        fz = __fmul_rn(__int2float_rn(cz), adaptive_step(q, 2));
     } else {
         fx = __fdiv_rn(__fmul_rn(__fmul_rn(__fadd_rn(__int2float_rn(cx), 0.5f), 2.0f), q.s), q.rdiv);
         fy = __fdiv_rn(__fmul_rn(__fmul_rn(__fadd_rn(__int2float_rn(cy), 0.5f), 2.0f), q.s), q.rdiv);

@@ -3,7 +3,8 @@
 //
 // Reference behaviour restated here (paths relative to the reference's source/):
 //   shift_points           preprocessor/shifting.hpp:11-36  (strict '<' scan from FLT_MAX)
-//   quantize               quantizer/truncated_octahedron_quantizer.hpp:21-55, cube_quantizer.hpp:15-27
+//   quantize               quantizer/truncated_octahedron_quantizer.hpp:21-55, cube_quantizer.hpp:15-27,
+//                          adaptive_quantizer.hpp:16-81
 //   ranges / direct switch composer/block_compressor.hpp:69-88
 //   error statistics       composer/block_compressor_rle.hpp:53-67
 //   block keys             quantizer/block_quantizer.hpp:93-115
@@ -46,21 +47,47 @@ __device__ void block_min3(unsigned long long m[3], unsigned long long* dst) {
     }
 }
 
+// Maximum over the block of three u32 order keys, then one atomicMax per axis.
+__device__ void block_max3(u32 m[3], unsigned int* dst) {
+    __shared__ u32 sm[3][kThreads / 32];
+    for (int a = 0; a < 3; ++a) {
+        u32 v = m[a];
+        for (int d = 16; d > 0; d >>= 1) v = max(v, __shfl_xor_sync(kFullMask, v, d));
+        if (lane_id() == 0) sm[a][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        u32 v = sm[threadIdx.x][0];
+        for (int w = 1; w < kThreads / 32; ++w) v = max(v, sm[threadIdx.x][w]);
+        atomicMax(&dst[threadIdx.x], v);
+    }
+}
+
 // shift_points keeps the first of equal minima; the key packs (order key, index) so the
 // smallest index wins ties (including +0 / -0), and the initial FLT_MAX candidate carries
-// index 0xffffffff.
+// index 0xffffffff.  The largest order key per axis feeds the adaptive quantizer's steps.
 __global__ void __launch_bounds__(kThreads) bbox_kernel(const float* __restrict__ xyz, u64 n, PointStats* stats) {
     unsigned long long m[3];
-    for (int a = 0; a < 3; ++a) m[a] = ~0ull;
+    u32 mx[3];
+    for (int a = 0; a < 3; ++a) {
+        m[a] = ~0ull;
+        mx[a] = 0u;
+    }
     const u64 stride = (u64)gridDim.x * kThreads;
     for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
         const float* p = xyz + 3 * i;
         for (int a = 0; a < 3; ++a) {
-            unsigned long long k = ((unsigned long long)order_key(__ldg(p + a)) << 32) | (u32)i;
-            m[a] = umin64(m[a], k);
+            const u32 ok = order_key(__ldg(p + a));
+            m[a] = umin64(m[a], ((unsigned long long)ok << 32) | (u32)i);
+            mx[a] = max(mx[a], ok);
         }
     }
     block_min3(m, stats->minkey);
+    block_max3(mx, stats->maxkey);
+}
+
+__device__ __forceinline__ float order_key_value(u32 k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
 __device__ __forceinline__ void load_offset(const float* xyz, const PointStats* st, float off[3]) {
@@ -75,6 +102,29 @@ __device__ __forceinline__ void load_offset(const float* xyz, const PointStats* 
 
 __device__ __forceinline__ bool finite3(float x, float y, float z) {
     return isfinite(x) && isfinite(y) && isfinite(z);
+}
+
+// AdaptiveQuantizer::quantize's steps (quantizer/adaptive_quantizer.hpp:42-64).  Over the
+// shifted points the minimum is 0 (the offset is the minimum) and the maximum is
+// max - offset (float subtraction is monotone), each compared against the scan's start
+// values (FLT_MAX, and the smallest normal float for the maxima).  One thread, IEEE
+// single-precision operations in the reference's order.
+__global__ void adaptive_steps_kernel(const float* __restrict__ xyz, float R, PointStats* stats) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float off[3];
+    load_offset(xyz, stats, off);
+    float d[3];
+    for (int a = 0; a < 3; ++a) {
+        const float hi = __fsub_rn(order_key_value(stats->maxkey[a]), off[a]);
+        const float mx = (FLT_MIN < hi) ? hi : FLT_MIN;
+        const float lo = __fsub_rn(off[a], off[a]);  // the minimum's own shifted value
+        const float mn = (lo < FLT_MAX) ? lo : FLT_MAX;
+        d[a] = __fsub_rn(mx, mn);
+    }
+    const float norm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])),
+                                            __fmul_rn(d[2], d[2])));
+    for (int a = 0; a < 3; ++a)
+        stats->step[a] = norm > 0.0f ? __fdiv_rn(__fmul_rn(R, d[a]), norm) : __fdiv_rn(R, __fsqrt_rn(3.0f));
 }
 
 __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* __restrict__ xyz, u64 n,
@@ -407,6 +457,9 @@ int grid_for(u64 n) {
 
 void launch_bbox(const float* xyz, uint64_t n, PointStats* stats, cudaStream_t st) {
     bbox_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, stats);
+}
+void launch_adaptive_steps(const float* xyz, float l2, PointStats* stats, cudaStream_t st) {
+    adaptive_steps_kernel<<<1, 32, 0, st>>>(xyz, l2, stats);
 }
 void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
                            cudaStream_t st) {

@@ -12,10 +12,12 @@ namespace xnyz {
 namespace dev {
 
 struct QuantParams {
-    int quantizer;  // 0 cube, 1 truncated octahedron
+    int quantizer;  // 0 cube, 1 truncated octahedron, 2 adaptive
     float div;      // float(double(2*l2)/sqrt(3|5))
     float s;        // l2 as float
     float rdiv;     // float(sqrt(3|5))
+    float step[3];  // adaptive: per-axis steps (decompression: from the container)
+    const float* step_dev;  // adaptive compression: the steps in device memory (PointStats::step)
 };
 
 // Results of the bounding-box / quantization sweeps (one struct in device memory).
@@ -28,6 +30,8 @@ struct PointStats {
     double mse_sum;                // sum of per-point squared errors
     unsigned int err;              // device error bits
     float offset[3];               // shift offset (written by quantize_range)
+    unsigned int maxkey[3];        // per axis: largest order key (bbox, for the adaptive steps)
+    float step[3];                 // adaptive quantizer steps (launch_adaptive_steps)
 };
 
 // Key layout of block mode.  Normal cells: key = id << 21 | quad << 18 | sfc18.  Cells with
@@ -94,6 +98,8 @@ struct EncodeTotals {
 
 // --- points ---------------------------------------------------------------------------
 void launch_bbox(const float* xyz, uint64_t n, PointStats* stats, cudaStream_t st);
+// AdaptiveQuantizer steps from the bounding box (after launch_bbox) into stats->step.
+void launch_adaptive_steps(const float* xyz, float l2, PointStats* stats, cudaStream_t st);
 void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
                            cudaStream_t st);
 void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, BlockKeyParams kp,
