@@ -133,6 +133,29 @@ def make_cloud(workload: str, n: int, seed: int):
     return S.terrain(n, seed)
 
 
+class RankSync:
+    """Barrier and max-over-ranks of a timing: one value per rank, the job's time is the
+    slowest rank's.  NCCL with a device tensor on GPUs, gloo with a host tensor elsewhere."""
+
+    def __init__(self, world: int, device=None):
+        self.world = world
+        self.device = device
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+
 # ------------------------------------------------------------------------------ GPU arm ---
 def run_gpu(args):
     import numpy as np
@@ -163,16 +186,9 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     variants = WORKLOADS[args.workload][2][: args.variants]
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    sync = RankSync(world, dev)
+    barrier = sync.barrier
+    max_over_ranks = sync.max
 
     # ---- device-resident step ----
     def device_step():
