@@ -247,41 +247,6 @@ __global__ void __launch_bounds__(kThreads) count_total_kernel(const i32* __rest
 }
 
 // ------------------------------------------------------------- recover units -------------
-__device__ __forceinline__ Seg shfl_up_seg(Seg v, int d) {
-    return Seg{__shfl_up_sync(kFullMask, v.head, d), __shfl_up_sync(kFullMask, v.sum, d)};
-}
-
-// Block-wide exclusive scan of Seg values.
-__device__ Seg block_exclusive_seg(Seg v, Seg* scratch, Seg& total) {
-    SegOp op;
-    const int w = threadIdx.x >> 5;
-    Seg inc = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const Seg o = shfl_up_seg(inc, d);
-        if ((int)lane_id() >= d) inc = op(o, inc);
-    }
-    if (lane_id() == 31) scratch[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        Seg x = (int)lane_id() < kThreads / 32 ? scratch[lane_id()] : Seg{0, 0};
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const Seg o = shfl_up_seg(x, d);
-            if ((int)lane_id() >= d) x = op(o, x);
-        }
-        if ((int)lane_id() < kThreads / 32) scratch[lane_id()] = x;
-    }
-    __syncthreads();
-    const Seg wp = w == 0 ? Seg{0, 0} : scratch[w - 1];
-    Seg ex = shfl_up_seg(inc, 1);
-    if (lane_id() == 0) ex = Seg{0, 0};
-    total = scratch[kThreads / 32 - 1];
-    const Seg r = op(wp, ex);
-    __syncthreads();
-    return r;
-}
-
 struct RecoverArgs {
     const u8* rep_sym;
     const u64* rep_patch;
@@ -305,14 +270,65 @@ struct RecoverArgs {
     u32* err;
 };
 
+// Warp-wide inclusive sums over the 32 lanes.
+template <typename T>
+__device__ __forceinline__ T warp_incl_add(T v) {
+    const u32 lane = lane_id();
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const T o = __shfl_up_sync(kFullMask, v, d);
+        if (lane >= (u32)d) v += o;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFullMask, v, d);
+    return v;
+}
+
+// Segmented inclusive sums over one round of 32 consecutive elements (lane order): lane i
+// gets the sum of v over [h, i] with h the last head lane at or before i, or carry plus the
+// sum over [0, i] when there is none (SegOp's semantics; carry = the running segment sum).
+template <typename T>
+__device__ __forceinline__ T warp_seg_incl(u32 heads, T v, T carry) {
+    const T incl = warp_incl_add(v);
+    const u32 le = heads & (lanemask_lt() | (1u << lane_id()));
+    const T before = __shfl_sync(kFullMask, incl - v, le ? 31 - __clz(le) : 0);
+    return le ? incl - before : carry + incl;
+}
+
+// Exclusive prefix over the block's warps of per-warp aggregates held in a[0..kWarps); the
+// tile total goes to a[kWarps].  One thread.
+template <typename T, typename Op>
+__device__ __forceinline__ void warps_exclusive(T* v, T identity, Op op) {
+    T run = identity;
+    for (int i = 0; i < kThreads / 32; ++i) {
+        const T x = v[i];
+        v[i] = run;
+        run = op(run, x);
+    }
+    v[kThreads / 32] = run;
+}
+
+// Warp w owns units [512 w, 512 w + 512) of the tile and takes them 32 at a time, one per
+// lane: staged symbols are read without bank conflicts, patches, counts and block starts
+// are read coalesced, and the points of a round are written to consecutive addresses.
+// Round 1 folds each warp's zero symbols, counts and quad / block segments, round 2 its
+// repos segments (or SFC sums); the block combines the warps, chained scans combine the
+// tiles, and the final pass rebuilds every running value with warp scans from its warp's
+// starting carry.
 template <bool DIRECT>
 __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) {
+    constexpr int kWarps = kThreads / 32;
     __shared__ u8 srep[kTile];
     __shared__ u8 squad[DIRECT ? 1 : kTile];
     __shared__ u8 sstart[DIRECT ? 1 : kTile];
-    __shared__ u64 scr64[16];
-    __shared__ Seg scrseg[16];
     __shared__ u32 slot;
+    __shared__ u64 wz[kWarps + 1], wc[kWarps + 1], wd[kWarps + 1];
+    __shared__ Seg wq[kWarps + 1], wb[kWarps + 1], wr[kWarps + 1];
     __shared__ u64 base_zero, base_count, base_sfc;
     __shared__ Seg base_quad, base_blk, base_rep;
     __shared__ u8 htab[256];
@@ -322,11 +338,15 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     const u64 base = (u64)tile * kTile;
     const u32 cnt = (u32)min((u64)kTile, a.units - base);
     const int tid = threadIdx.x;
+    const int w = tid >> 5;
+    const u32 lane = lane_id();
+    const u32 lt = lanemask_lt();
+    const bool has_val = a.rep_val != nullptr;
     for (int i = tid; i < 256; i += kThreads) htab[i] = a.hinv ? a.hinv[i] : 0;
     for (int i = 0; i < kItems; ++i) {
         const u32 e = (u32)i * kThreads + tid;
         if (e < cnt) {
-            srep[e] = a.rep_val ? (u8)1 : a.rep_sym[base + e];
+            srep[e] = has_val ? (u8)1 : a.rep_sym[base + e];
             if (!DIRECT) {
                 squad[e] = a.quad_sym[base + e];
                 sstart[e] = a.is_start[base + e];
@@ -334,101 +354,128 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         }
     }
     __syncthreads();
-    const u32 e0 = (u32)tid * kItems;
     const bool rle = a.rp.rle != 0;
-
-    // ---- round 1: zero symbols, quad segments, block carry, counts ----
-    u64 zr = 0, csum = 0;
-    Seg qs{0, 0}, bs{0, 0};
+    const u32 wfirst = (u32)w * (32u * kItems);
     SegOp op;
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = e0 + i;
-        if (e >= cnt) break;
-        zr += !a.rep_val && srep[e] == 0;
-        if (rle) csum += (u64)max(a.counts[base + e], 0);
-        if (!DIRECT) {
-            const bool st = sstart[e] != 0;
-            qs = op(qs, Seg{st ? 1ull : 0ull, (u64)(squad[e] ? squad[e] - 1u : 0u)});
-            bs = op(bs, Seg{st ? 1ull : 0ull, st ? (u64)a.start_block[base + e] : 0ull});
+
+    // repos value of unit e; zc: index of the warp's next patch (advanced on symbol 0).
+    // Called by all lanes (it votes).
+    auto rep_value = [&](u32 e, bool valid, u64& zc) -> u64 {
+        const u32 sym = valid ? srep[e] : 1u;
+        const u32 zb = __ballot_sync(kFullMask, valid && !has_val && sym == 0u);
+        const u64 z = zc + __popc(zb & lt);
+        zc += __popc(zb);
+        if (!valid) return 0;
+        if (has_val) return a.rep_val[base + e];
+        if (sym) return sym - 1u;
+        if (z < a.npatch) return a.rep_patch[z];
+        atomicOr(a.err, kErrBadStream);
+        return 0;
+    };
+
+    // ---- round 1: zero symbols, counts, quad and block segments per warp ----
+    {
+        u64 z = 0, c = 0, bc = 0;
+        u32 qc = 0;
+        bool any_head = false;
+        for (int r = 0; r < kItems; ++r) {
+            const u32 e = wfirst + (u32)r * 32u + lane;
+            const bool valid = e < cnt;
+            z += __popc(__ballot_sync(kFullMask, valid && !has_val && srep[e] == 0));
+            if (rle && valid) c += (u64)max(a.counts[base + e], 0);
+            if (!DIRECT) {
+                const bool st = valid && sstart[e] != 0;
+                const u32 hm = __ballot_sync(kFullMask, st);
+                const u32 qd = valid ? squad[e] : 1u;
+                qc = __shfl_sync(kFullMask, warp_seg_incl<u32>(hm, qd ? qd - 1u : 0u, qc), 31);
+                const u32 bv = st ? a.start_block[base + e] : 0u;
+                const u32 last = __shfl_sync(kFullMask, bv, hm ? 31 - __clz(hm) : 0);
+                if (hm) bc = last;
+                any_head |= hm != 0;
+            }
+        }
+        c = warp_sum(c);
+        if (lane == 0) {
+            wz[w] = z;
+            wc[w] = c;
+            wq[w] = Seg{any_head ? 1ull : 0ull, (u64)qc};
+            wb[w] = Seg{any_head ? 1ull : 0ull, bc};
         }
     }
-    u64 tz, tc;
-    const u64 ez = block_exclusive<kThreads>(zr, 0ull, AddOp{}, scr64, tz);
-    const u64 ec = block_exclusive<kThreads>(csum, 0ull, AddOp{}, scr64, tc);
-    Seg tq{0, 0}, tb{0, 0}, eq{0, 0}, eb{0, 0};
-    if (!DIRECT) {
-        eq = block_exclusive_seg(qs, scrseg, tq);
-        eb = block_exclusive_seg(bs, scrseg, tb);
+    __syncthreads();
+    if (tid == 0) {
+        warps_exclusive(wz, 0ull, AddOp{});
+        warps_exclusive(wc, 0ull, AddOp{});
+        if (!DIRECT) {
+            warps_exclusive(wq, Seg{0, 0}, op);
+            warps_exclusive(wb, Seg{0, 0}, op);
+        }
     }
+    __syncthreads();
     // one warp per chained scan
-    const int wid = tid >> 5;
-    if (wid == 0) {
+    if (w == 0) {
         LookBack64 l{a.flag, a.agg, a.inc};
-        const u64 r = warp_lookback_add(l, tile, tz, a.err);
+        const u64 r = warp_lookback_add(l, tile, wz[kWarps], a.err);
         if (tid == 0) base_zero = r;
-    } else if (wid == 1 && rle) {
+    } else if (w == 1 && rle) {
         LookBack64 l{a.flag + ntiles, a.agg + 2ull * ntiles, a.inc + 2ull * ntiles};
-        const u64 r = warp_lookback_add(l, tile, tc, a.err);
+        const u64 r = warp_lookback_add(l, tile, wc[kWarps], a.err);
         if (tid == 32) base_count = r;
-    } else if (wid == 2 && !DIRECT) {
+    } else if (w == 2 && !DIRECT) {
         Seg* ag = reinterpret_cast<Seg*>(a.agg + 4ull * ntiles);
         Seg* in = reinterpret_cast<Seg*>(a.inc + 4ull * ntiles);
-        const Seg r =
-            warp_lookback(a.flag + 2 * ntiles, ag, in, tile, tq, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+        const Seg r = warp_lookback(a.flag + 2 * ntiles, ag, in, tile, wq[kWarps], Seg{0, 0}, SegOp{}, LoadSeg{},
+                                    StoreSeg{}, a.err);
         if (tid == 64) base_quad = r;
-    } else if (wid == 3 && !DIRECT) {
+    } else if (w == 3 && !DIRECT) {
         Seg* ag = reinterpret_cast<Seg*>(a.agg + 6ull * ntiles);
         Seg* in = reinterpret_cast<Seg*>(a.inc + 6ull * ntiles);
-        const Seg r =
-            warp_lookback(a.flag + 3 * ntiles, ag, in, tile, tb, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+        const Seg r = warp_lookback(a.flag + 3 * ntiles, ag, in, tile, wb[kWarps], Seg{0, 0}, SegOp{}, LoadSeg{},
+                                    StoreSeg{}, a.err);
         if (tid == 96) base_blk = r;
     }
     if (!rle && tid == 0) base_count = 0;
     __syncthreads();
 
-    // ---- round 2: repos values (need the patch index) -> repos segments / SFC sums ----
-    // repos value of element e; zrun: index of the next patch (advanced on symbol 0).  The
-    // values are produced here and again in the final loop (patches re-read through L1)
-    // rather than kept in a per-thread array.
-    auto rep_value = [&](u32 e, u64& zrun) -> u64 {
-        if (a.rep_val) return a.rep_val[base + e];
-        const u32 sym = srep[e];
-        if (sym) return sym - 1u;
-        const u64 z = zrun++;
-        if (z < a.npatch) return a.rep_patch[z];
-        atomicOr(a.err, kErrBadStream);
-        return 0;
-    };
-    const u64 zrun0 = base_zero + ez;
-    u64 zrun = zrun0;
-    Seg rs{0, 0};
-    u64 dsum = 0;
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = e0 + i;
-        if (e >= cnt) continue;
-        const u64 v = rep_value(e, zrun);
-        if (DIRECT) {
-            dsum += v;
-        } else {
-            const bool st = sstart[e] != 0;
-            const bool qchange = squad[e] != 1;  // quad delta != 0
-            rs = op(rs, Seg{(st || qchange) ? 1ull : 0ull, v});
+    // ---- round 2: repos segments (block mode) or SFC sums (direct mode) per warp ----
+    {
+        u64 zc = base_zero + wz[w];
+        u64 d = 0, rc = 0;
+        bool any_head = false;
+        for (int r = 0; r < kItems; ++r) {
+            const u32 e = wfirst + (u32)r * 32u + lane;
+            const bool valid = e < cnt;
+            const u64 v = rep_value(e, valid, zc);
+            if (DIRECT) {
+                d += v;
+            } else {
+                const u32 hm = __ballot_sync(kFullMask, valid && (sstart[e] != 0 || squad[e] != 1));
+                rc = __shfl_sync(kFullMask, warp_seg_incl<u64>(hm, v, rc), 31);
+                any_head |= hm != 0;
+            }
+        }
+        if (DIRECT) d = warp_sum(d);
+        if (lane == 0) {
+            wd[w] = d;
+            wr[w] = Seg{any_head ? 1ull : 0ull, rc};
         }
     }
-    u64 td = 0, ed = 0;
-    Seg tr{0, 0}, er{0, 0};
-    if (DIRECT) ed = block_exclusive<kThreads>(dsum, 0ull, AddOp{}, scr64, td);
-    else er = block_exclusive_seg(rs, scrseg, tr);
-    if (wid == 0) {
+    __syncthreads();
+    if (tid == 0) {
+        if (DIRECT) warps_exclusive(wd, 0ull, AddOp{});
+        else warps_exclusive(wr, Seg{0, 0}, op);
+    }
+    __syncthreads();
+    if (w == 0) {
         if (DIRECT) {
             LookBack64 l{a.flag + 4 * ntiles, a.agg + 8ull * ntiles, a.inc + 8ull * ntiles};
-            const u64 r = warp_lookback_add(l, tile, td, a.err);
+            const u64 r = warp_lookback_add(l, tile, wd[kWarps], a.err);
             if (tid == 0) base_sfc = r;
         } else {
             Seg* ag = reinterpret_cast<Seg*>(a.agg + 8ull * ntiles);
             Seg* in = reinterpret_cast<Seg*>(a.inc + 8ull * ntiles);
-            const Seg r =
-                warp_lookback(a.flag + 4 * ntiles, ag, in, tile, tr, Seg{0, 0}, SegOp{}, LoadSeg{}, StoreSeg{}, a.err);
+            const Seg r = warp_lookback(a.flag + 4 * ntiles, ag, in, tile, wr[kWarps], Seg{0, 0}, SegOp{}, LoadSeg{},
+                                        StoreSeg{}, a.err);
             if (tid == 0) base_rep = r;
         }
     }
@@ -436,61 +483,79 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
 
     // ---- final: coordinates, recover, unshift, expand ----
     const QuantParams q = a.rp.q;
-    // -rle: output position from the count prefix; -normal: one point per unit.
-    u64 opos = rle ? base_count + ec : base + e0;
-    u64 sfc = base_sfc + ed;
-    Seg qrun = op(base_quad, eq), brun = op(base_blk, eb), rrun = op(base_rep, er);
-    zrun = zrun0;
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = e0 + i;
-        if (e >= cnt) break;
-        const u64 rv = rep_value(e, zrun);
-        i32 cx, cy, cz;
+    u64 zc = base_zero + wz[w];
+    u64 oc = base_count + wc[w];  // -rle: output position of the warp's first point
+    u64 scar = DIRECT ? base_sfc + wd[w] : 0ull;
+    u32 qcar = DIRECT ? 0u : (u32)op(base_quad, wq[w]).sum;
+    u64 bcar = DIRECT ? 0ull : op(base_blk, wb[w]).sum;
+    u64 rcar = DIRECT ? 0ull : op(base_rep, wr[w]).sum;
+    for (int r = 0; r < kItems; ++r) {
+        const u32 e = wfirst + (u32)r * 32u + lane;
+        const bool valid = e < cnt;
+        const u64 rv = rep_value(e, valid, zc);
+        i32 cx = 0, cy = 0, cz = 0;
         if (DIRECT) {
-            sfc += rv;
+            const u64 sfc = scar + warp_incl_add(rv);
+            scar = __shfl_sync(kFullMask, sfc, 31);
             const u64 m = a.rp.hilbert ? hilbert_apply(htab, sfc, a.rp.bits, 0u) : sfc;
             cx = (i32)gather3(m);
             cy = (i32)gather3(m >> 1);
             cz = (i32)gather3(m >> 2);
         } else {
-            const bool st = sstart[e] != 0;
-            qrun = op(qrun, Seg{st ? 1ull : 0ull, (u64)(squad[e] ? squad[e] - 1u : 0u)});
-            brun = op(brun, Seg{st ? 1ull : 0ull, st ? (u64)a.start_block[base + e] : 0ull});
-            rrun = op(rrun, Seg{(st || squad[e] != 1) ? 1ull : 0ull, rv});
-            const u64 quadj = qrun.sum, reposj = rrun.sum, b = brun.sum;
-            if (squad[e] == 0) atomicOr(a.err, kErrBadStream);  // quad patches never occur
-            const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
-            const u64 nx = a.rp.nx, ny = a.rp.ny;
-            const u64 pbx = (blk % nx * 2) * 64, pby = (blk / nx % ny * 2) * 64, pbz = (blk / nx / ny * 2) * 64;
-            u64 m = reposj;
-            if (a.rp.hilbert)
-                m = reposj < (1ull << 18) ? hilbert_apply(htab, reposj, 5, a.rp.hstart_inv)
-                                          : hilbert_apply(htab, reposj, 20, 0u);
-            cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64 + (u64)gather3(m));
-            cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gather3(m >> 1));
-            cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gather3(m >> 2));
+            const bool st = valid && sstart[e] != 0;
+            const u32 qd = valid ? squad[e] : 1u;
+            const u32 hm = __ballot_sync(kFullMask, st);
+            const u32 quadj = warp_seg_incl<u32>(hm, qd ? qd - 1u : 0u, qcar);
+            qcar = __shfl_sync(kFullMask, quadj, 31);
+            const u32 bv = st ? a.start_block[base + e] : 0u;
+            const u32 le = hm & (lt | (1u << lane));
+            const u32 bsel = __shfl_sync(kFullMask, bv, le ? 31 - __clz(le) : 0);
+            const u64 b = le ? (u64)bsel : bcar;
+            bcar = __shfl_sync(kFullMask, b, 31);
+            const u32 hr = __ballot_sync(kFullMask, valid && (st || qd != 1u));
+            const u64 reposj = warp_seg_incl<u64>(hr, rv, rcar);
+            rcar = __shfl_sync(kFullMask, reposj, 31);
+            if (valid) {
+                if (qd == 0) atomicOr(a.err, kErrBadStream);  // quad patches never occur
+                const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
+                const u64 nx = a.rp.nx, ny = a.rp.ny;
+                const u64 pbx = (blk % nx * 2) * 64, pby = (blk / nx % ny * 2) * 64, pbz = (blk / nx / ny * 2) * 64;
+                u64 m = reposj;
+                if (a.rp.hilbert)
+                    m = reposj < (1ull << 18) ? hilbert_apply(htab, reposj, 5, a.rp.hstart_inv)
+                                              : hilbert_apply(htab, reposj, 20, 0u);
+                cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64 + (u64)gather3(m));
+                cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gather3(m >> 1));
+                cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gather3(m >> 2));
+            }
         }
+        // -rle: output position from the count prefix; -normal and cells: one per unit.
+        u64 c = 1, opos = base + e;
+        if (rle) {
+            c = valid ? (u64)max(a.counts[base + e], 0) : 0ull;
+            const u64 incl = warp_incl_add(c);
+            opos = oc + incl - c;
+            oc += __shfl_sync(kFullMask, incl, 31);
+        }
+        if (!valid) continue;  // after the round's warp-wide votes and shuffles
         if (a.rp.cells) {
             i32* co = reinterpret_cast<i32*>(a.out);
             co[3 * opos] = cx;
             co[3 * opos + 1] = cy;
             co[3 * opos + 2] = cz;
-            ++opos;
             continue;
         }
         float x, y, z;
         recover(q, cx, cy, cz, a.rp.off[0], a.rp.off[1], a.rp.off[2], x, y, z);
-        const u64 c = rle ? (u64)max(a.counts[base + e], 0) : 1ull;
         if (opos + c > a.nout) {
             atomicOr(a.err, kErrOverflow);
-            break;
+            continue;
         }
-        for (u64 r = 0; r < c; ++r) {
-            a.out[3 * (opos + r)] = x;
-            a.out[3 * (opos + r) + 1] = y;
-            a.out[3 * (opos + r) + 2] = z;
+        for (u64 k = 0; k < c; ++k) {
+            a.out[3 * (opos + k)] = x;
+            a.out[3 * (opos + k) + 1] = y;
+            a.out[3 * (opos + k) + 2] = z;
         }
-        opos += c;
     }
 }
 
