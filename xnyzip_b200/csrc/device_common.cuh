@@ -54,6 +54,50 @@ struct AddOp {
     __device__ __forceinline__ T operator()(T a, T b) const { return a + b; }
 };
 
+// Warp-wide inclusive sums over the 32 lanes.
+template <typename T>
+__device__ __forceinline__ T warp_incl_add(T v) {
+    const u32 lane = lane_id();
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const T o = __shfl_up_sync(kFullMask, v, d);
+        if (lane >= (u32)d) v += o;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFullMask, v, d);
+    return v;
+}
+
+// Segmented inclusive sums over one round of 32 consecutive elements (lane order): lane i
+// gets the sum of v over [h, i] with h the last head lane at or before i, or carry plus the
+// sum over [0, i] when there is none (SegOp's semantics; carry = the running segment sum).
+template <typename T>
+__device__ __forceinline__ T warp_seg_incl(u32 heads, T v, T carry) {
+    const T incl = warp_incl_add(v);
+    const u32 le = heads & (lanemask_lt() | (1u << lane_id()));
+    const T before = __shfl_sync(kFullMask, incl - v, le ? 31 - __clz(le) : 0);
+    return le ? incl - before : carry + incl;
+}
+
+// Exclusive prefix over the block's warps of per-warp aggregates held in v[0..WARPS); the
+// tile total goes to v[WARPS].  One thread.
+template <int WARPS, typename T, typename Op>
+__device__ __forceinline__ void warps_exclusive(T* v, T identity, Op op) {
+    T run = identity;
+    for (int i = 0; i < WARPS; ++i) {
+        const T x = v[i];
+        v[i] = run;
+        run = op(run, x);
+    }
+    v[WARPS] = run;
+}
+
+
 // Block-wide exclusive scan (THREADS a multiple of 32, <= 1024).  `total` receives the
 // block aggregate.  `scratch` holds THREADS/32 + 1 elements of shared memory.
 template <int THREADS, typename T, typename Op>

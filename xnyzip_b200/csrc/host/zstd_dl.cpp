@@ -2,6 +2,7 @@
 
 #include <dlfcn.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <mutex>
 
@@ -20,11 +21,32 @@ struct Api {
     unsigned long long (*content_size)(const void*, size_t) = nullptr;
     unsigned (*is_error)(size_t) = nullptr;
     const char* (*error_name)(size_t) = nullptr;
+    // explicit contexts: ZSTD_compressCCtx / ZSTD_decompressDCtx give the same bytes as
+    // ZSTD_compress / ZSTD_decompress (which build and free a context per call)
+    void* (*create_cctx)(void) = nullptr;
+    size_t (*free_cctx)(void*) = nullptr;
+    size_t (*compress_cctx)(void*, void*, size_t, const void*, size_t, int) = nullptr;
+    void* (*create_dctx)(void) = nullptr;
+    size_t (*free_dctx)(void*) = nullptr;
+    size_t (*decompress_dctx)(void*, void*, size_t, const void*, size_t) = nullptr;
     void* handle = nullptr;
 };
 
 Api g_api;
 std::mutex g_mu;
+std::atomic<bool> g_loaded{false};
+
+// One compression and one decompression context per host thread, kept for the thread's
+// lifetime (the batch workers compress thousands of frames each).
+struct ThreadContexts {
+    void* c = nullptr;
+    void* d = nullptr;
+    ~ThreadContexts() {
+        if (c && g_api.free_cctx) g_api.free_cctx(c);
+        if (d && g_api.free_dctx) g_api.free_dctx(d);
+    }
+};
+thread_local ThreadContexts t_ctx;
 constexpr unsigned kWantVersion = 10507;  // 1.5.7
 
 bool load_locked(const char* path, std::string& err) {
@@ -50,6 +72,14 @@ bool load_locked(const char* path, std::string& err) {
     a.content_size = reinterpret_cast<unsigned long long (*)(const void*, size_t)>(dlsym(h, "ZSTD_getFrameContentSize"));
     a.is_error = reinterpret_cast<unsigned (*)(size_t)>(dlsym(h, "ZSTD_isError"));
     a.error_name = reinterpret_cast<const char* (*)(size_t)>(dlsym(h, "ZSTD_getErrorName"));
+    a.create_cctx = reinterpret_cast<void* (*)(void)>(dlsym(h, "ZSTD_createCCtx"));
+    a.free_cctx = reinterpret_cast<size_t (*)(void*)>(dlsym(h, "ZSTD_freeCCtx"));
+    a.compress_cctx =
+        reinterpret_cast<size_t (*)(void*, void*, size_t, const void*, size_t, int)>(dlsym(h, "ZSTD_compressCCtx"));
+    a.create_dctx = reinterpret_cast<void* (*)(void)>(dlsym(h, "ZSTD_createDCtx"));
+    a.free_dctx = reinterpret_cast<size_t (*)(void*)>(dlsym(h, "ZSTD_freeDCtx"));
+    a.decompress_dctx =
+        reinterpret_cast<size_t (*)(void*, void*, size_t, const void*, size_t)>(dlsym(h, "ZSTD_decompressDCtx"));
     if (!a.version || !a.bound || !a.compress || !a.decompress || !a.content_size || !a.is_error || !a.error_name) {
         err = p + " lacks the zstd entry points";
         dlclose(h);
@@ -62,6 +92,7 @@ bool load_locked(const char* path, std::string& err) {
     }
     a.handle = h;
     g_api = a;
+    g_loaded.store(true, std::memory_order_release);
     return true;
 }
 
@@ -77,6 +108,7 @@ bool zstd_load(const char* path, std::string& err) {
 }
 
 bool zstd_available(std::string& err) {
+    if (g_loaded.load(std::memory_order_acquire)) return true;
     std::lock_guard<std::mutex> lk(g_mu);
     return load_locked(nullptr, err);
 }
@@ -86,7 +118,9 @@ size_t zstd_bound(size_t n) { return g_api.bound ? g_api.bound(n) : 0; }
 bool zstd_compress_into(const uint8_t* src, size_t n, int level, uint8_t* dst, size_t cap, size_t& written,
                         std::string& err) {
     if (!zstd_available(err)) return false;
-    const size_t r = g_api.compress(dst, cap, src, n, level);
+    if (!t_ctx.c && g_api.create_cctx && g_api.compress_cctx) t_ctx.c = g_api.create_cctx();
+    const size_t r = t_ctx.c ? g_api.compress_cctx(t_ctx.c, dst, cap, src, n, level)
+                             : g_api.compress(dst, cap, src, n, level);
     if (g_api.is_error(r)) {
         err = g_api.error_name(r);
         return false;
@@ -121,7 +155,9 @@ bool zstd_content_size(const uint8_t* src, size_t n, uint64_t& size, std::string
 
 bool zstd_decompress(const uint8_t* src, size_t n, uint8_t* dst, uint64_t dst_size, std::string& err) {
     if (!zstd_available(err)) return false;
-    const size_t r = g_api.decompress(dst, dst_size, src, n);
+    if (!t_ctx.d && g_api.create_dctx && g_api.decompress_dctx) t_ctx.d = g_api.create_dctx();
+    const size_t r = t_ctx.d ? g_api.decompress_dctx(t_ctx.d, dst, dst_size, src, n)
+                             : g_api.decompress(dst, dst_size, src, n);
     if (g_api.is_error(r)) {
         err = g_api.error_name(r);
         return false;

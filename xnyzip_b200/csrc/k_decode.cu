@@ -107,40 +107,6 @@ __device__ __forceinline__ Tri shfl_down_t(Tri v, int d) {
 __device__ __forceinline__ Tri shfl_t(Tri v, int l) {
     return Tri{__shfl_sync(kFullMask, v.a, l), __shfl_sync(kFullMask, v.n, l), __shfl_sync(kFullMask, v.b, l)};
 }
-__device__ __forceinline__ Tri shfl_up_tri(Tri v, int d) {
-    return Tri{__shfl_up_sync(kFullMask, v.a, d), __shfl_up_sync(kFullMask, v.n, d), __shfl_up_sync(kFullMask, v.b, d)};
-}
-
-// Block-wide exclusive scan of Tri values (thread order).
-__device__ Tri block_exclusive_tri(Tri v, Tri* scratch, Tri& total) {
-    TriOp op;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Tri inc = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const Tri o = shfl_up_tri(inc, d);
-        if (lane >= d) inc = op(o, inc);
-    }
-    if (lane == 31) scratch[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        Tri x = lane < kThreads / 32 ? scratch[lane] : Tri{0, 0, 0};
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const Tri o = shfl_up_tri(x, d);
-            if (lane >= d) x = op(o, x);
-        }
-        if (lane < kThreads / 32) scratch[lane] = x;
-    }
-    __syncthreads();
-    const Tri wp = w == 0 ? Tri{0, 0, 0} : scratch[w - 1];
-    Tri ex = shfl_up_tri(inc, 1);
-    if (lane == 0) ex = Tri{0, 0, 0};
-    total = scratch[kThreads / 32 - 1];
-    const Tri r = op(wp, ex);
-    __syncthreads();
-    return r;
-}
 
 __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __restrict__ wb, u64 bb, int width_b,
                                                                  const u32* __restrict__ wc, u64 bc, int width_c,
@@ -148,64 +114,83 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
                                                                  u8* __restrict__ is_start, u32* __restrict__ start_block,
                                                                  LookBackState lb, u32* tile_counter,
                                                                  unsigned long long* count_total, u32* err) {
-    __shared__ u64 scr64[16];
-    __shared__ Tri scrtri[16];
+    constexpr int kWarps = kThreads / 32;
     __shared__ u32 slot;
+    __shared__ u64 wsb[kWarps + 1];
+    __shared__ Tri wtc[kWarps + 1];
     __shared__ u64 base_b;
     __shared__ Tri base_c;
     const u32 tile = claim_tile(tile_counter, &slot);
     const u32 ntiles = gridDim.x;
     const int tid = threadIdx.x;
-    const u64 first = (u64)tile * kTile + (u64)tid * kItems;  // my blocks: first .. first + kItems - 1
+    const int w = tid >> 5;
+    const u32 lane = lane_id();
+    // warp w owns blocks [512 w, 512 w + 512) of the tile, 32 consecutive blocks per round
+    const u64 wfirst = (u64)tile * kTile + (u64)w * (32u * kItems);
     const u64 mb = width_b >= 64 ? ~0ull : ((1ull << width_b) - 1), mc = width_c >= 64 ? ~0ull : ((1ull << width_c) - 1);
-    // the deltas are unpacked twice (the words stay in L1) rather than held in registers
     auto delta_b = [&](u64 j) { return width_b ? (peek_lsb64(wb, bb + j * (u64)width_b) & mb) : 0ull; };
     auto delta_c = [&](u64 j) { return width_c ? (peek_lsb64(wc, bc + j * (u64)width_c) & mc) : 0ull; };
-    u64 sb = 0, sc = 0, spc = 0;
-    u32 cnt = 0;
-    for (int i = 0; i < kItems; ++i) {
-        const u64 j = first + i;
-        if (j >= nb) break;
-        sb += delta_b(j);
-        sc += delta_c(j);
-        spc += sc;  // sum of the thread-local inclusive prefixes of the count deltas
-        ++cnt;
+
+    // Running values along the warp's blocks: blk (block id), cnt (block count = inclusive
+    // sum of the count deltas), start (first unit of the block = exclusive sum of the
+    // counts).  One pass from zero gives the warp's aggregates, the second from the true
+    // carries writes the outputs.
+    auto pass = [&](u64& blk, u64& cnt, u64& start, bool write) {
+        for (int r = 0; r < kItems; ++r) {
+            const u64 j = wfirst + (u64)r * 32u + lane;
+            const bool valid = j < nb;
+            const u64 db = valid ? delta_b(j) : 0ull, dc = valid ? delta_c(j) : 0ull;
+            const u64 bj = blk + warp_incl_add(db);
+            const u64 cj = cnt + warp_incl_add(dc);
+            const u64 vc = valid ? cj : 0ull;
+            const u64 ci = warp_incl_add(vc);
+            const u64 sj = start + ci - vc;
+            blk = __shfl_sync(kFullMask, bj, 31);
+            cnt = __shfl_sync(kFullMask, cj, 31);
+            start += __shfl_sync(kFullMask, ci, 31);
+            if (write && valid) {
+                blk_out[j] = bj;
+                if (cj > 0 && sj < units) {  // non-empty block (the reference skips empty ones)
+                    is_start[sj] = 1;
+                    start_block[sj] = (u32)j;
+                }
+            }
+        }
+    };
+    {
+        u64 blk = 0, cnt = 0, start = 0;
+        pass(blk, cnt, start, false);
+        const u64 wbeg = wfirst < nb ? wfirst : nb;
+        const u64 nvalid = (nb - wbeg) < 32u * kItems ? nb - wbeg : 32u * kItems;
+        if (lane == 0) {
+            wsb[w] = blk;
+            wtc[w] = Tri{cnt, nvalid, start};
+        }
     }
-    u64 tb;
-    const u64 eb = block_exclusive<kThreads>(sb, 0ull, AddOp{}, scr64, tb);
-    Tri tt;
-    const Tri ec = block_exclusive_tri(Tri{sc, (u64)cnt, spc}, scrtri, tt);
+    __syncthreads();
+    if (tid == 0) {
+        warps_exclusive<kWarps>(wsb, 0ull, AddOp{});
+        warps_exclusive<kWarps>(wtc, Tri{0, 0, 0}, TriOp{});
+    }
+    __syncthreads();
     if (tid < 32) {
         LookBack64 l{lb.flag, lb.agg, lb.inc};
-        const u64 r = warp_lookback_add(l, tile, tb, err);
+        const u64 r = warp_lookback_add(l, tile, wsb[kWarps], err);
         if (tid == 0) base_b = r;
     } else if (tid < 64) {
         Tri* ag = reinterpret_cast<Tri*>(lb.agg + ntiles);
         Tri* in = reinterpret_cast<Tri*>(lb.inc + ntiles);
-        const Tri r = warp_lookback(lb.flag + ntiles, ag, in, tile, tt, Tri{0, 0, 0}, TriOp{}, LoadTri{}, StoreTri{}, err);
+        const Tri r = warp_lookback(lb.flag + ntiles, ag, in, tile, wtc[kWarps], Tri{0, 0, 0}, TriOp{}, LoadTri{},
+                                    StoreTri{}, err);
         if (tid == 32) {
             base_c = r;
-            if (tile == ntiles - 1) *count_total = TriOp{}(r, tt).b;
+            if (tile == ntiles - 1) *count_total = TriOp{}(r, wtc[kWarps]).b;
         }
     }
     __syncthreads();
-    u64 blk = base_b + eb;
-    const Tri pre = TriOp{}(base_c, ec);
-    u64 cntv = pre.a;   // count delta sum so far: inclusive scan gives the block counts
-    u64 start = pre.b;  // sum of the counts so far: the first unit of my first block
-    for (int i = 0; i < kItems; ++i) {
-        const u64 j = first + i;
-        if (j >= nb) break;
-        blk += delta_b(j);
-        cntv += delta_c(j);
-        blk_out[j] = blk;
-        const u64 en = start + cntv;
-        if (en > start && start < units) {  // non-empty block (the reference skips empty ones)
-            is_start[start] = 1;
-            start_block[start] = (u32)j;
-        }
-        start = en;
-    }
+    const Tri pre = TriOp{}(base_c, wtc[w]);
+    u64 blk = base_b + wsb[w], cnt = pre.a, start = pre.b;
+    pass(blk, cnt, start, true);
 }
 
 // ---------------------------------------------------------------- units --------------
@@ -269,49 +254,6 @@ struct RecoverArgs {
     float* out;
     u32* err;
 };
-
-// Warp-wide inclusive sums over the 32 lanes.
-template <typename T>
-__device__ __forceinline__ T warp_incl_add(T v) {
-    const u32 lane = lane_id();
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const T o = __shfl_up_sync(kFullMask, v, d);
-        if (lane >= (u32)d) v += o;
-    }
-    return v;
-}
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFullMask, v, d);
-    return v;
-}
-
-// Segmented inclusive sums over one round of 32 consecutive elements (lane order): lane i
-// gets the sum of v over [h, i] with h the last head lane at or before i, or carry plus the
-// sum over [0, i] when there is none (SegOp's semantics; carry = the running segment sum).
-template <typename T>
-__device__ __forceinline__ T warp_seg_incl(u32 heads, T v, T carry) {
-    const T incl = warp_incl_add(v);
-    const u32 le = heads & (lanemask_lt() | (1u << lane_id()));
-    const T before = __shfl_sync(kFullMask, incl - v, le ? 31 - __clz(le) : 0);
-    return le ? incl - before : carry + incl;
-}
-
-// Exclusive prefix over the block's warps of per-warp aggregates held in a[0..kWarps); the
-// tile total goes to a[kWarps].  One thread.
-template <typename T, typename Op>
-__device__ __forceinline__ void warps_exclusive(T* v, T identity, Op op) {
-    T run = identity;
-    for (int i = 0; i < kThreads / 32; ++i) {
-        const T x = v[i];
-        v[i] = run;
-        run = op(run, x);
-    }
-    v[kThreads / 32] = run;
-}
 
 // Warp w owns units [512 w, 512 w + 512) of the tile and takes them 32 at a time, one per
 // lane: staged symbols are read without bank conflicts, patches, counts and block starts
@@ -404,11 +346,11 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     }
     __syncthreads();
     if (tid == 0) {
-        warps_exclusive(wz, 0ull, AddOp{});
-        warps_exclusive(wc, 0ull, AddOp{});
+        warps_exclusive<kThreads / 32>(wz, 0ull, AddOp{});
+        warps_exclusive<kThreads / 32>(wc, 0ull, AddOp{});
         if (!DIRECT) {
-            warps_exclusive(wq, Seg{0, 0}, op);
-            warps_exclusive(wb, Seg{0, 0}, op);
+            warps_exclusive<kThreads / 32>(wq, Seg{0, 0}, op);
+            warps_exclusive<kThreads / 32>(wb, Seg{0, 0}, op);
         }
     }
     __syncthreads();
@@ -462,8 +404,8 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     }
     __syncthreads();
     if (tid == 0) {
-        if (DIRECT) warps_exclusive(wd, 0ull, AddOp{});
-        else warps_exclusive(wr, Seg{0, 0}, op);
+        if (DIRECT) warps_exclusive<kThreads / 32>(wd, 0ull, AddOp{});
+        else warps_exclusive<kThreads / 32>(wr, Seg{0, 0}, op);
     }
     __syncthreads();
     if (w == 0) {

@@ -365,28 +365,37 @@ __global__ void __launch_bounds__(kThreads) gr_encode_kernel(const u64* __restri
     u32 tile;
     u64 base;
     const u32 cnt = stage_tile(vals, n, sv, &slot, tile_counter, tile, base);
-    const u32 e0 = threadIdx.x * kItems;
+    // warp w owns elements [512 w, 512 w + 512), one per lane per round: the codewords of a
+    // round are consecutive in the stream, so the lanes' bits merge into few words
+    const u32 lane = lane_id(), wfirst = (threadIdx.x >> 5) * (32u * kItems);
     u64 sum = 0;
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
-        if (e0 + i < cnt) sum += (sv[e0 + i] >> k) + 1u + (u64)k;
+    for (int r = 0; r < kItems; ++r) {
+        const u32 e = wfirst + (u32)r * 32u + lane;
+        if (e < cnt) sum += (sv[e] >> k) + 1u + (u64)k;
+    }
     u64 tot;
     const u64 ex = block_exclusive<kThreads>(sum, 0ull, AddOp{}, scratch, tot);
-    u64 pos = tile_bit_base(lb, tile, tot, &sbase, total_bits, err) + ex;
+    u64 wpos0 = tile_bit_base(lb, tile, tot, &sbase, total_bits, err) + __shfl_sync(kFullMask, ex, 0);
     const u64 mask = k ? ((1ull << k) - 1) : 0ull;
 #pragma unroll 1
-    for (int i = 0; i < kItems; ++i) {
-        const bool ok = e0 + i < cnt;
-        const u64 v = ok ? sv[e0 + i] : 0ull;
+    for (int r = 0; r < kItems; ++r) {
+        const u32 e = wfirst + (u32)r * 32u + lane;
+        const bool ok = e < cnt;
+        const u64 v = ok ? sv[e] : 0ull;
         const u64 q = v >> k;
+        const u64 len = ok ? q + 1u + (u64)k : 0ull;
+        const u64 incl = warp_incl_add(len);
+        const u64 pos = wpos0 + incl - len;
+        wpos0 += __shfl_sync(kFullMask, incl, 31);
         u64 wval = 0, wpos = pos;
         u32 nb = 0;
-        if (ok && pos + q + 1u + (u64)k > cap_bits) {  // output bound (never reached with valid sizes)
+        if (ok && pos + len > cap_bits) {  // output bound (never reached with valid sizes)
             atomicOr(err, kErrOverflow);
         } else if (ok) {
-            if (q + 1u + (u64)k <= 64u) {
+            if (len <= 64u) {
                 wval = ((q ? ((1ull << q) - 1) : 0ull)) | ((v & mask) << (q + 1));
-                nb = (u32)(q + 1 + k);
+                nb = (u32)len;
             } else {
                 write_ones_lsb(words, pos, q);  // long unary run, written by this lane alone
                 wval = (v & mask) << 1;
@@ -395,7 +404,6 @@ __global__ void __launch_bounds__(kThreads) gr_encode_kernel(const u64* __restri
             }
         }
         warp_write_lsb(words, wpos, wval, nb);
-        if (ok) pos += q + 1u + (u64)k;
     }
 }
 
