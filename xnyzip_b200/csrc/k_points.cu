@@ -21,6 +21,30 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Grid-stride loop over points that issues the loads of U points (U strides apart) before
+// processing them, so that each thread keeps U loads in flight.  body(i, x, y, z).
+template <int U, typename F>
+__device__ __forceinline__ void for_each_point(const float* __restrict__ xyz, u64 n, F&& body) {
+    const u64 stride = (u64)gridDim.x * kThreads;
+    for (u64 i0 = (u64)blockIdx.x * kThreads + threadIdx.x; i0 < n; i0 += U * stride) {
+        float x[U], y[U], z[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const u64 i = i0 + (u64)u * stride;
+            if (i < n) {
+                x[u] = __ldg(xyz + 3 * i);
+                y[u] = __ldg(xyz + 3 * i + 1);
+                z[u] = __ldg(xyz + 3 * i + 2);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const u64 i = i0 + (u64)u * stride;
+            if (i < n) body(i, x[u], y[u], z[u]);
+        }
+    }
+}
+
 // Order key of a float for the minimum scan: monotone in value, +0 and -0 equal, NaN last.
 __device__ __forceinline__ u32 order_key(float f) {
     u32 b = __float_as_uint(f);
@@ -73,15 +97,14 @@ __global__ void __launch_bounds__(kThreads) bbox_kernel(const float* __restrict_
         m[a] = ~0ull;
         mx[a] = 0u;
     }
-    const u64 stride = (u64)gridDim.x * kThreads;
-    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-        const float* p = xyz + 3 * i;
+    for_each_point<4>(xyz, n, [&](u64 i, float x, float y, float z) {
+        const float v[3] = {x, y, z};
         for (int a = 0; a < 3; ++a) {
-            const u32 ok = order_key(__ldg(p + a));
+            const u32 ok = order_key(v[a]);
             m[a] = umin64(m[a], ((unsigned long long)ok << 32) | (u32)i);
             mx[a] = max(mx[a], ok);
         }
-    }
+    });
     block_min3(m, stats->minkey);
     block_max3(mx, stats->maxkey);
 }
@@ -146,12 +169,10 @@ __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* _
     u32 nonfinite = 0;
     float emax = 0.0f;
     double esum = 0.0;
-    const u64 stride = (u64)gridDim.x * kThreads;
-    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-        const float x = __ldg(xyz + 3 * i), y = __ldg(xyz + 3 * i + 1), z = __ldg(xyz + 3 * i + 2);
+    for_each_point<4>(xyz, n, [&](u64, float x, float y, float z) {
         if (!finite3(x, y, z)) {
             ++nonfinite;
-            continue;
+            return;
         }
         const float px = __fsub_rn(x, ox), py = __fsub_rn(y, oy), pz = __fsub_rn(z, oz);
         i32 c[3];
@@ -169,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* _
             emax = fmaxf(emax, e);
             esum += (double)e;
         }
-    }
+    });
     for (int d = 16; d > 0; d >>= 1) {
         for (int a = 0; a < 3; ++a) {
             mx[a] = max(mx[a], __shfl_xor_sync(kFullMask, mx[a], d));
@@ -256,18 +277,15 @@ __global__ void __launch_bounds__(kThreads) keys_block_kernel(const float* __res
     for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0;
     __syncthreads();
     DigitHist dh{sh, passes};
-    const u64 stride = (u64)gridDim.x * kThreads;
-    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-        const float px = __fsub_rn(__ldg(xyz + 3 * i), off[0]);
-        const float py = __fsub_rn(__ldg(xyz + 3 * i + 1), off[1]);
-        const float pz = __fsub_rn(__ldg(xyz + 3 * i + 2), off[2]);
+    for_each_point<4>(xyz, n, [&](u64 i, float fx, float fy, float fz) {
+        const float px = __fsub_rn(fx, off[0]), py = __fsub_rn(fy, off[1]), pz = __fsub_rn(fz, off[2]);
         i32 x, y, z;
         quantize(q, px, py, pz, x, y, z);
         const u64 k = block_key(x, y, z, kp, htab);
         keys[i] = k;
         if (payload) payload[i] = (u32)i;
         if (passes) dh.add(k);
-    }
+    });
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += kThreads)
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
@@ -388,11 +406,8 @@ __global__ void __launch_bounds__(kThreads) keys_direct_kernel(const float* __re
     for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0;
     __syncthreads();
     DigitHist dh{sh, passes};
-    const u64 stride = (u64)gridDim.x * kThreads;
-    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-        const float px = __fsub_rn(__ldg(xyz + 3 * i), off[0]);
-        const float py = __fsub_rn(__ldg(xyz + 3 * i + 1), off[1]);
-        const float pz = __fsub_rn(__ldg(xyz + 3 * i + 2), off[2]);
+    for_each_point<4>(xyz, n, [&](u64 i, float fx, float fy, float fz) {
+        const float px = __fsub_rn(fx, off[0]), py = __fsub_rn(fy, off[1]), pz = __fsub_rn(fz, off[2]);
         i32 x, y, z;
         quantize(q, px, py, pz, x, y, z);
         u64 m = morton3(x, y, z);
@@ -401,7 +416,7 @@ __global__ void __launch_bounds__(kThreads) keys_direct_kernel(const float* __re
         keys[i] = k;
         if (payload) payload[i] = (u32)i;
         if (passes) dh.add(k);
-    }
+    });
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += kThreads)
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
