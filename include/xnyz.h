@@ -117,6 +117,23 @@ xnyz_status xnyz_compress(xnyz_ctx* ctx, const float* xyz, uint64_t n, int xyz_i
 xnyz_status xnyz_compress_device(xnyz_ctx* ctx, const float* xyz, uint64_t n, const xnyz_params* params,
                                  const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info);
 
+/* Shared codebooks <- BlockCompressor<float>::fit_profile / compress_with_profile
+ * (composer/block_compressor.hpp:241-431) and the profile blob of serialize_profile /
+ * deserialize_profile (composer/block_encoding_profile.hpp:17-72): [u32 LE length][repos
+ * Huffman meta][u32 LE length][quad Huffman meta].  Both write the -normal container in block
+ * mode whatever the ranges (params->rle must be 0, direct_threshold is ignored) and reject
+ * the extended container.  xnyz_fit_profile builds Huffman codes that cover every symbol
+ * 0..255 (build_complete) and returns the container plus a malloc'd profile (free with
+ * xnyz_free); xnyz_compress_with_profile codes with the profile's codebooks (load_meta) and
+ * returns XNYZ_ERR_INVALID_ARG for an empty or malformed profile.  Frames decode with
+ * xnyz_decompress as usual.  sort_order as in xnyz_compress. */
+xnyz_status xnyz_fit_profile(xnyz_ctx* ctx, const float* xyz, uint64_t n, int xyz_is_device, const xnyz_params* params,
+                             int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order, uint8_t** profile,
+                             uint64_t* profile_len);
+xnyz_status xnyz_compress_with_profile(xnyz_ctx* ctx, const float* xyz, uint64_t n, int xyz_is_device,
+                                       const xnyz_params* params, const uint8_t* profile, uint64_t profile_len,
+                                       int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order);
+
 /* Decompress.  `in` is host memory holding a zstd frame (is_zstd = 1) or a raw container.
  * quantizer / l2_bound / rle must be the values used to compress (the container does not
  * record them, exactly as in the reference).  The result is written to a malloc'd host

@@ -82,6 +82,31 @@ class Oracle(_Lib):
         data = self.take(out, ln.value).tobytes()
         return (data, order[: n if n else 0]) if with_order else data
 
+    def fit_profile(self, xyz, quantizer, l2, hilbert, zstd=True):
+        """fit_profile (block_compressor.hpp:241-246): (frame, serialized profile)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        out, ln, pr, pl = _u8p(), C.c_uint64(), _u8p(), C.c_uint64()
+        rc = self.fn("fit_profile", [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_int, C.c_int, C.POINTER(_u8p),
+                                     C.POINTER(C.c_uint64), C.POINTER(_u8p), C.POINTER(C.c_uint64)])(
+            _buf(xyz), xyz.shape[0], QUANT.get(quantizer, quantizer), l2, int(hilbert), 3 if zstd else -1,
+            C.byref(out), C.byref(ln), C.byref(pr), C.byref(pl))
+        if rc:
+            raise RuntimeError(f"orc_fit_profile failed ({rc})")
+        return self.take(out, ln.value).tobytes(), self.take(pr, pl.value).tobytes()
+
+    def compress_with_profile(self, xyz, quantizer, l2, hilbert, profile, zstd=True):
+        """compress_with_profile (block_compressor.hpp:248-256): the frame."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        pb = np.frombuffer(bytes(profile), dtype=np.uint8)
+        out, ln = _u8p(), C.c_uint64()
+        rc = self.fn("compress_with_profile", [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_int, C.c_void_p,
+                                               C.c_uint64, C.c_int, C.POINTER(_u8p), C.POINTER(C.c_uint64)])(
+            _buf(xyz), xyz.shape[0], QUANT.get(quantizer, quantizer), l2, int(hilbert), _buf(pb), pb.size,
+            3 if zstd else -1, C.byref(out), C.byref(ln))
+        if rc:
+            raise RuntimeError(f"orc_compress_with_profile failed ({rc})")
+        return self.take(out, ln.value).tobytes()
+
     def decompress(self, buf, quantizer, l2, rle, zstd=True):
         b = np.frombuffer(buf, dtype=np.uint8)
         out, n = _f32p(), C.c_uint64()
@@ -173,6 +198,31 @@ class Reference(Oracle):
             raise RuntimeError("ref_compress failed")
         data = self.take(out, ln.value).tobytes()
         return (data, srt) if with_sorted else data
+
+    def fit_profile(self, xyz, quantizer, l2, hilbert, direct_threshold=1024):
+        """BlockCompressor::fit_profile: (zstd frame, serialize_profile blob)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        out, ln, pr, pl = _u8p(), C.c_uint64(), _u8p(), C.c_uint64()
+        rc = self.fn("fit_profile", [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_int, C.c_int, C.POINTER(_u8p),
+                                     C.POINTER(C.c_uint64), C.POINTER(_u8p), C.POINTER(C.c_uint64), C.c_void_p])(
+            _buf(xyz), xyz.shape[0], QUANT.get(quantizer, quantizer), l2, int(hilbert), direct_threshold,
+            C.byref(out), C.byref(ln), C.byref(pr), C.byref(pl), None)
+        if rc:
+            raise RuntimeError("ref_fit_profile failed")
+        return self.take(out, ln.value).tobytes(), self.take(pr, pl.value).tobytes()
+
+    def compress_with_profile(self, xyz, quantizer, l2, hilbert, profile, direct_threshold=1024):
+        """BlockCompressor::compress_with_profile(deserialize_profile(profile)): the frame."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        pb = np.frombuffer(bytes(profile), dtype=np.uint8)
+        out, ln = _u8p(), C.c_uint64()
+        rc = self.fn("compress_with_profile", [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_int, C.c_int,
+                                               C.c_void_p, C.c_uint64, C.POINTER(_u8p), C.POINTER(C.c_uint64)])(
+            _buf(xyz), xyz.shape[0], QUANT.get(quantizer, quantizer), l2, int(hilbert), direct_threshold, _buf(pb),
+            pb.size, C.byref(out), C.byref(ln))
+        if rc:
+            raise RuntimeError("ref_compress_with_profile failed")
+        return self.take(out, ln.value).tobytes()
 
     def decompress(self, buf, quantizer, l2, rle):
         b = np.frombuffer(buf, dtype=np.uint8)

@@ -97,6 +97,43 @@ int ref_compress(const float* xyz, uint64_t n, int quantizer, float l2, int hilb
     }
 }
 
+// BlockCompressor::fit_profile: the zstd frame and serialize_profile of the profile.
+int ref_fit_profile(const float* xyz, uint64_t n, int quantizer, float l2, int hilbert, int direct_threshold,
+                    uint8_t** out, uint64_t* out_len, uint8_t** prof, uint64_t* prof_len, float* sorted_xyz) {
+    try {
+        auto pts = to_points(xyz, n);
+        XnYZip::BlockCompressor<float> c(qtype(quantizer), l2, false, direct_threshold);
+        auto [bytes, profile] = c.fit_profile(pts, hilbert != 0);
+        const auto blob = XnYZip::serialize_profile(profile);
+        if (sorted_xyz)
+            for (uint64_t i = 0; i < n; ++i)
+                for (int k = 0; k < 3; ++k) sorted_xyz[3 * i + k] = pts[i][k];
+        *out = dup_bytes(bytes, out_len);
+        *prof = dup_bytes(blob, prof_len);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_fit_profile: %s\n", e.what());
+        return 1;
+    }
+}
+
+// BlockCompressor::compress_with_profile with deserialize_profile(blob).
+int ref_compress_with_profile(const float* xyz, uint64_t n, int quantizer, float l2, int hilbert,
+                              int direct_threshold, const uint8_t* prof, uint64_t prof_len, uint8_t** out,
+                              uint64_t* out_len) {
+    try {
+        auto pts = to_points(xyz, n);
+        XnYZip::BlockCompressor<float> c(qtype(quantizer), l2, false, direct_threshold);
+        const auto profile = XnYZip::deserialize_profile(std::vector<uint8_t>(prof, prof + prof_len));
+        auto bytes = c.compress_with_profile(pts, hilbert != 0, profile);
+        *out = dup_bytes(bytes, out_len);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_compress_with_profile: %s\n", e.what());
+        return 1;
+    }
+}
+
 int ref_decompress(const uint8_t* buf, uint64_t len, int quantizer, float l2, int rle, float** xyz_out,
                    uint64_t* n_out) {
     try {

@@ -509,6 +509,10 @@ struct Huff {
             egk = best_k(d);
             return;
         }
+        from_freq(freq);
+    }
+    // build_from_freq (:91-123)
+    void from_freq(const std::unordered_map<T, u64>& freq) {
         auto cmp = [](const std::shared_ptr<Node>& a, const std::shared_ptr<Node>& b) { return a->freq > b->freq; };
         std::priority_queue<std::shared_ptr<Node>, std::vector<std::shared_ptr<Node>>, decltype(cmp)> pq(cmp);
         for (auto& kv : freq) {
@@ -529,6 +533,57 @@ struct Huff {
             pq.push(p);
         }
         walk(pq.top(), 0u, 0);
+    }
+    // build_complete (:70-85): the data's frequencies, every missing value of [0, amax] with
+    // frequency 1, built without the exp-Golomb switch.
+    void build_complete(const std::vector<T>& d, T amax) {
+        table.clear();
+        eg = false;
+        egk = 0;
+        std::unordered_map<T, u64> freq;
+        for (T v : d) freq[v]++;
+        for (T s = 0; s <= amax; ++s) {
+            if (freq.find(s) == freq.end()) freq[s] = 1;
+            if (s == std::numeric_limits<T>::max()) break;
+        }
+        from_freq(freq);
+    }
+    // load_meta (:172-203): entries inserted in the meta's order.
+    void load_meta(const Bytes& m) {
+        table.clear();
+        eg = false;
+        egk = 0;
+        size_t p = 0;
+        if (m.size() >= 4 && m[0] == 0xE1 && m[1] == 0xC1 && m[2] == 0x01) {
+            p = 4;
+            if (m[3] == 0x01) {
+                egk = m.size() > 4 ? m[4] : 0;
+                eg = true;
+                return;
+            }
+        }
+        auto be32 = [&]() {
+            if (p + 4 > m.size()) throw std::runtime_error("truncated Huffman meta");
+            u32 v = (u32(m[p]) << 24) | (u32(m[p + 1]) << 16) | (u32(m[p + 2]) << 8) | u32(m[p + 3]);
+            p += 4;
+            return v;
+        };
+        const u32 count = be32();
+        for (u32 i = 0; i < count; ++i) {
+            if (p + sizeof(T) + 5 > m.size()) throw std::runtime_error("truncated Huffman meta");
+            T sym;
+            if constexpr (sizeof(T) == 8) {
+                u64 v = 0;
+                for (int k = 0; k < 8; ++k) v = (v << 8) | m[p++];
+                sym = static_cast<T>(v);
+            } else {
+                std::memcpy(&sym, m.data() + p, sizeof(T));
+                p += sizeof(T);
+            }
+            const u8 l = m[p++];
+            const u32 b = be32();
+            table[sym] = Code{b, l};
+        }
     }
     // get_meta (:126-146): u32 BE count; per entry symbol (u64 BE, else native bytes),
     // u8 len, u32 BE bits.  exp-Golomb: E1 C1 01 01 k.
@@ -749,6 +804,24 @@ void huff_stream(Writer& w, const std::vector<T>& sym) {
     w.stream(h.meta(), h.encode(sym));
 }
 
+// Shared codebooks of compress_internal (composer/block_compressor.hpp:271-431): mode 1
+// builds complete codebooks and records their metas, mode 2 loads the given metas.
+struct Share {
+    int mode = 0;
+    Bytes rep_in, quad_in;    // mode 2
+    Bytes rep_out, quad_out;  // mode 1
+};
+
+template <typename T>
+void huff_stream_shared(Writer& w, const std::vector<T>& sym, Share& sh, bool repos) {
+    Huff<T> h;
+    if (sh.mode == 2) h.load_meta(repos ? sh.rep_in : sh.quad_in);
+    else h.build_complete(sym, static_cast<T>(255));
+    const Bytes m = h.meta();
+    if (sh.mode == 1) (repos ? sh.rep_out : sh.quad_out) = m;
+    w.stream(m, h.encode(sym));
+}
+
 struct Cell {
     i32 x, y, z;
 };
@@ -814,7 +887,7 @@ void lcp_streams(const std::vector<Rec>& rec, Lcp& m) {
 // BlockCompressor::compress (composer/block_compressor.hpp:39-222) and
 // BlockCompressorRLE::compress (composer/block_compressor_rle.hpp:38-321).
 Bytes compress_container(const float* xyz, u64 n, int quantizer, float l2, bool hil, bool rle, int thresh,
-                         std::vector<u64>* order) {
+                         std::vector<u64>* order, Share* share = nullptr) {
     float off[3];
     std::vector<i32> q;
     std::vector<float> params;
@@ -863,7 +936,7 @@ Bytes compress_container(const float* xyz, u64 n, int quantizer, float l2, bool 
     w.pod<i32>(ry);
     w.pod<i32>(rz);
     int mr = std::max({rx, ry, rz});
-    bool direct = mr < thresh;
+    bool direct = !share && mr < thresh;  // shared codebooks: always block mode
     w.pod<bool>(hil);
     w.pod<bool>(direct);
     std::vector<u64> perm(m);
@@ -906,13 +979,15 @@ Bytes compress_container(const float* xyz, u64 n, int quantizer, float l2, bool 
         Bytes gm, gd;
         gr_pack(pat, gm, gd);
         w.stream(gm, gd);
-        huff_stream(w, sym);
+        if (share) huff_stream_shared(w, sym, *share, true);
+        else huff_stream(w, sym);
         std::vector<u8> qs;
         std::vector<u64> qp;
         pfd(L.quads, qs, qp);
         gr_pack(qp, gm, gd);  // GolombRiceCoder<uint8_t>: same bits for values < 256
         w.stream(gm, gd);
-        huff_stream(w, qs);
+        if (share) huff_stream_shared(w, qs, *share, false);
+        else huff_stream(w, qs);
     }
     if (rle) {
         std::vector<int> sc(m);
@@ -1070,6 +1145,64 @@ int orc_compress(const float* xyz, uint64_t n, int quantizer, float l2, int hilb
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "orc_compress: %s\n", e.what());
+        return 1;
+    }
+}
+
+// fit_profile / compress_with_profile (composer/block_compressor.hpp:241-256), -normal; the
+// profile in serialize_profile's layout (composer/block_encoding_profile.hpp:34-48).
+static int finish_frame(Bytes& c, int zstd_level, uint8_t** out, uint64_t* out_len) {
+    if (zstd_level >= 0) {
+        if (!zstd_load()) return 3;
+        Bytes z(g_zstd.compressBound(c.size()));
+        size_t zs = g_zstd.compress(z.data(), z.size(), c.data(), c.size(), zstd_level);
+        if (g_zstd.isError(zs)) return 4;
+        z.resize(zs);
+        c.swap(z);
+    }
+    *out = dup(c, out_len);
+    return 0;
+}
+
+int orc_fit_profile(const float* xyz, uint64_t n, int quantizer, float l2, int hilbert, int zstd_level, uint8_t** out,
+                    uint64_t* out_len, uint8_t** prof, uint64_t* prof_len) {
+    try {
+        Share sh;
+        sh.mode = 1;
+        Bytes c = compress_container(xyz, n, quantizer, l2, hilbert != 0, false, 1024, nullptr, &sh);
+        Bytes blob;
+        for (const Bytes* m : {&sh.rep_out, &sh.quad_out}) {
+            const u32 len = static_cast<u32>(m->size());
+            for (int b = 0; b < 4; ++b) blob.push_back(u8(len >> (8 * b)));
+            blob.insert(blob.end(), m->begin(), m->end());
+        }
+        *prof = dup(blob, prof_len);
+        return finish_frame(c, zstd_level, out, out_len);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "orc_fit_profile: %s\n", e.what());
+        return 1;
+    }
+}
+
+int orc_compress_with_profile(const float* xyz, uint64_t n, int quantizer, float l2, int hilbert, const uint8_t* prof,
+                              uint64_t prof_len, int zstd_level, uint8_t** out, uint64_t* out_len) {
+    try {
+        Share sh;
+        sh.mode = 2;
+        uint64_t p = 0;
+        for (Bytes* m : {&sh.rep_in, &sh.quad_in}) {
+            if (p + 4 > prof_len) throw std::runtime_error("malformed profile");
+            const u32 len = u32(prof[p]) | (u32(prof[p + 1]) << 8) | (u32(prof[p + 2]) << 16) | (u32(prof[p + 3]) << 24);
+            p += 4;
+            if (len > prof_len - p) throw std::runtime_error("malformed profile");
+            m->assign(prof + p, prof + p + len);
+            p += len;
+        }
+        if (sh.rep_in.empty() || sh.quad_in.empty()) throw std::runtime_error("empty profile");
+        Bytes c = compress_container(xyz, n, quantizer, l2, hilbert != 0, false, 1024, nullptr, &sh);
+        return finish_frame(c, zstd_level, out, out_len);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "orc_compress_with_profile: %s\n", e.what());
         return 1;
     }
 }

@@ -84,6 +84,24 @@ def main():
     out["config1/frame_len"] = np.array([len(frame)], np.int64)
     out["config1/decoded_sha256"] = np.frombuffer(hashlib.sha256(dec.tobytes()).digest(), np.uint8)
     out["config1/input_sha256"] = np.frombuffer(hashlib.sha256(x.tobytes()).digest(), np.uint8)
+    # shared codebooks (block_compressor.hpp:241-431): a profile fit on one terrain chunk,
+    # then two other chunks (one with a range below the direct threshold) coded with it
+    fit_x = S.terrain(3000, 31, extent=300.0, amplitude=3.0, wavelength=150.0)
+    others = [S.terrain(2500, 32, extent=300.0, amplitude=3.0, wavelength=150.0),
+              np.random.default_rng(33).uniform(0, 3, (1200, 3)).astype(np.float32)]
+    ref.quiet(True)
+    try:
+        fit_frame, prof = ref.fit_profile(fit_x, "to", 0.05, 1)
+        with_frames = [ref.compress_with_profile(x, "to", 0.05, 1, prof) for x in others]
+    finally:
+        ref.quiet(False)
+    out["profile/fit_points"] = fit_x
+    out["profile/fit_frame"] = np.frombuffer(fit_frame, np.uint8)
+    out["profile/profile"] = np.frombuffer(prof, np.uint8)
+    for i, (x, fr) in enumerate(zip(others, with_frames)):
+        out[f"profile/points{i}"] = x
+        out[f"profile/frame{i}"] = np.frombuffer(fr, np.uint8)
+    print(f"profile: {len(prof)} B profile, frames {len(fit_frame)} / {[len(f) for f in with_frames]} B")
     out["names"] = np.array(names)
     np.savez_compressed(os.path.join(HERE, "reference_fixtures.npz"), **out)
     print("config1:", len(frame), "B frame")

@@ -87,7 +87,9 @@ def test_chunk_driver_flags():
     with pytest.raises(SystemExit):
         D.parse_compress_args(["--input", "x", "--output-dir", "o", "--mode", "mapreduce"])
     with pytest.raises(SystemExit):
-        D.parse_compress_args(["--input", "x", "--output-dir", "o", "--shared-codebook"])
+        D.parse_compress_args(["--input", "x", "--output-dir", "o", "--shared-codebook", "--mode", "-rle"])
+    assert D.parse_compress_args(["--input", "x", "--output-dir", "o", "--shared-codebook"]).shared_codebook
+    assert D.QUANTIZERS["adaptive"] == D.QUANTIZERS["to"] == 1  # as the reference driver's compress_block
     a = D.parse_compress_args(["--input", "x", "--output-dir", "o", "--block-size", "120", "--quantizer", "adaptive",
                                "--curve", "-h", "--mode", "-rle", "--bound", "0.5"])
     assert (a.block_size, a.quantizer, a.curve, a.mode, a.bound) == (120, "adaptive", "-h", "-rle", 0.5)
@@ -120,3 +122,44 @@ def test_bench_max_over_ranks():
     mp.start_processes(_sync_worker, args=(2, _free_port(), q), nprocs=2, join=True, start_method="spawn")
     got = sorted(q.get() for _ in range(2))
     assert got == [(0, 2.5), (1, 2.5)]
+
+
+def _fake_profile_compress(clouds, prof):
+    if clouds is None:  # the fit on block 0: a profile that names the block's bytes
+        return b"P" + zlib.compress(np.ascontiguousarray(prof, np.float32).tobytes())[:16]
+    return [prof + zlib.compress(np.ascontiguousarray(c, np.float32).tobytes()) for c in clouds]
+
+
+def _shared_worker(rank, world, port, path, outdir):
+    _env(rank, world, port)
+    from xnyzip_b200 import chunk_driver as D
+    dist = D._Dist()
+    try:
+        args = D.parse_compress_args(["--input", path, "--output-dir", outdir, "--block-size", str(12 * 700),
+                                      "--shared-codebook"])
+        D.compress_file(args, dist, compressor=_fake_profile_compress, log=lambda *a: None)
+    finally:
+        dist.close()
+
+
+def test_chunk_driver_shared_codebook_two_ranks(tmp_path):
+    """Every block of every rank is coded with the profile rank 0 fit on block 0."""
+    from xnyzip_b200 import chunk_driver as D
+    x = np.random.default_rng(8).random((5000, 3), dtype=np.float32)
+    path = str(tmp_path / "pts.bin")
+    x.tofile(path)
+    outdir = str(tmp_path / "out")
+    mp.start_processes(_shared_worker, args=(2, _free_port(), path, outdir), nprocs=2, join=True,
+                       start_method="spawn")
+    want = _fake_profile_compress(None, x[:700])
+    seen = 0
+    for r in (0, 1):
+        part = open(os.path.join(outdir, D.part_name(r)), "rb").read()
+        for line in open(os.path.join(outdir, D.manifest_name(r))):
+            rec = json.loads(line)
+            fr = part[rec["part_offset"]:rec["part_offset"] + rec["compressed_size"]]
+            assert fr.startswith(want)
+            seen += 1
+    assert seen == 8
+    summ = json.load(open(os.path.join(outdir, "summary.json")))
+    assert summ["shared_codebook"] is True and summ["warmup_s"] > 0

@@ -98,3 +98,29 @@ def test_oracle_gr_and_bitpack_vs_reference(oracle, reference):
         assert oracle.gr_pack(d) == reference.gr_pack(d)
         if d.size:
             assert oracle.bitpack(d) == reference.bitpack(d)
+
+
+def test_oracle_shared_codebook_fixture(oracle):
+    """fit_profile / compress_with_profile (composer/block_compressor.hpp:241-431): the
+    restatement reproduces the reference's frames and profile bytes."""
+    f = np.load(GOLDEN)
+    frame, prof = oracle.fit_profile(f["profile/fit_points"], "to", 0.05, 1)
+    assert frame == f["profile/fit_frame"].tobytes()
+    assert prof == f["profile/profile"].tobytes()
+    for i in range(2):
+        got = oracle.compress_with_profile(f[f"profile/points{i}"], "to", 0.05, 1, prof)
+        assert got == f[f"profile/frame{i}"].tobytes()
+
+
+def test_oracle_shared_codebook_vs_reference(oracle, reference):
+    from xnyzip_b200 import synthetic as S
+    fit_x = S.terrain(6000, 51, extent=300.0, amplitude=3.0, wavelength=150.0)
+    others = [S.uniform(4000, 52), S.spheres(5000, 12, 53, extent=150.0)]
+    for q in ("to", "cube", "adaptive"):
+        for hil in (0, 1):
+            a = oracle.fit_profile(fit_x, q, 0.1, hil)
+            b = quiet_call(reference, reference.fit_profile, fit_x, q, 0.1, hil)
+            assert a == b, (q, hil)
+            for x in others:
+                assert oracle.compress_with_profile(x, q, 0.1, hil, b[1]) == \
+                    quiet_call(reference, reference.compress_with_profile, x, q, 0.1, hil, b[1]), (q, hil)

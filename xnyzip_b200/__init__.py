@@ -95,6 +95,50 @@ class Context:
         self.last_info = info
         return (data, order[:n]) if want_order else data
 
+    @staticmethod
+    def _host_points(points):
+        if _is_torch_cuda(points):
+            pts = points.contiguous()
+            return pts, pts.numel() // 3, C.c_void_p(pts.data_ptr()), 1
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        return pts, pts.shape[0], pts.ctypes.data_as(C.c_void_p), 0
+
+    def fit_profile(self, points, quantizer: int, l2: float, hilbert: bool, use_zstd: bool = True,
+                    want_order: bool = False):
+        """BlockCompressor::fit_profile (xnyz_fit_profile): (frame, profile[, order]); the
+        profile is the serialize_profile blob of the complete codebooks."""
+        prm = Params(int(quantizer), float(l2), int(bool(hilbert)), 0, 1024)
+        pts, n, ptr, on_dev = self._host_points(points)
+        out, ln = C.POINTER(C.c_uint8)(), C.c_uint64()
+        prof, pl = C.POINTER(C.c_uint8)(), C.c_uint64()
+        order = np.zeros(max(n, 1), dtype=np.uint64) if want_order else None
+        N.check(N.fit_profile(self.handle, ptr, n, on_dev, C.byref(prm), int(use_zstd), C.byref(out), C.byref(ln),
+                              order.ctypes.data_as(C.c_void_p) if want_order else None, C.byref(prof), C.byref(pl)))
+        try:
+            data, blob = C.string_at(out, ln.value), C.string_at(prof, pl.value)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+            N.free(C.cast(prof, C.c_void_p))
+        return (data, blob, order[:n]) if want_order else (data, blob)
+
+    def compress_with_profile(self, points, quantizer: int, l2: float, hilbert: bool, profile: bytes,
+                              use_zstd: bool = True, want_order: bool = False):
+        """BlockCompressor::compress_with_profile (xnyz_compress_with_profile)."""
+        prm = Params(int(quantizer), float(l2), int(bool(hilbert)), 0, 1024)
+        pts, n, ptr, on_dev = self._host_points(points)
+        blob = np.frombuffer(bytes(profile), dtype=np.uint8)
+        out, ln = C.POINTER(C.c_uint8)(), C.c_uint64()
+        order = np.zeros(max(n, 1), dtype=np.uint64) if want_order else None
+        N.check(N.compress_with_profile(self.handle, ptr, n, on_dev, C.byref(prm),
+                                        blob.ctypes.data_as(C.c_void_p) if blob.size else None, blob.size,
+                                        int(use_zstd), C.byref(out), C.byref(ln),
+                                        order.ctypes.data_as(C.c_void_p) if want_order else None))
+        try:
+            data = C.string_at(out, ln.value)
+        finally:
+            N.free(C.cast(out, C.c_void_p))
+        return (data, order[:n]) if want_order else data
+
     def decompress(self, data: bytes, quantizer: int, l2: float, rle: bool, is_zstd: bool = True,
                    out: np.ndarray | None = None) -> np.ndarray:
         """Decoded points as an (n, 3) float32 array.  With `out` (e.g. a view of pinned
@@ -356,6 +400,27 @@ class _CompressorBase:
 class BlockCompressor(_CompressorBase):
     """composer/block_compressor.hpp:31-39 (-normal container)."""
     _rle = False
+
+    def _reorder(self, points, order):
+        if isinstance(points, np.ndarray):
+            view = points.reshape(-1, 3)
+            view[:] = view[order.astype(np.int64)]
+
+    def fit_profile(self, points, curve_type: bool):
+        """block_compressor.hpp:241-246: (zstd frame, profile); reorders a numpy `points`
+        array into container order like compress()."""
+        ctx = self.ctx or default_context()
+        data, prof, order = ctx.fit_profile(points, self.quantizer, self.l2_bound, bool(curve_type), want_order=True)
+        self._reorder(points, order)
+        return data, prof
+
+    def compress_with_profile(self, points, curve_type: bool, profile: bytes) -> bytes:
+        """block_compressor.hpp:248-256."""
+        ctx = self.ctx or default_context()
+        data, order = ctx.compress_with_profile(points, self.quantizer, self.l2_bound, bool(curve_type), profile,
+                                                want_order=True)
+        self._reorder(points, order)
+        return data
 
 
 class BlockCompressorRLE(_CompressorBase):

@@ -69,6 +69,10 @@ trim = _proto("xnyz_trim", [_p])
 free = _proto("xnyz_free", [_p], None)
 compress = _proto("xnyz_compress", [_p, _p, C.c_uint64, C.c_int, C.POINTER(Params), C.c_int, _u8pp,
                                     C.POINTER(C.c_uint64), _p, C.POINTER(CompressInfo)])
+fit_profile = _proto("xnyz_fit_profile", [_p, _p, C.c_uint64, C.c_int, C.POINTER(Params), C.c_int, _u8pp,
+                                          C.POINTER(C.c_uint64), _p, _u8pp, C.POINTER(C.c_uint64)])
+compress_with_profile = _proto("xnyz_compress_with_profile", [_p, _p, C.c_uint64, C.c_int, C.POINTER(Params), _p,
+                                                              C.c_uint64, C.c_int, _u8pp, C.POINTER(C.c_uint64), _p])
 compress_device = _proto("xnyz_compress_device", [_p, _p, C.c_uint64, C.POINTER(Params), C.POINTER(_p),
                                                   C.POINTER(C.c_uint64), C.POINTER(CompressInfo)])
 decompress = _proto("xnyz_decompress", [_p, _p, C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_int,
@@ -135,7 +139,7 @@ EXPORTED = [
     "xnyz_create", "xnyz_destroy", "xnyz_last_error", "xnyz_version", "xnyz_set_zstd_library", "xnyz_host_alloc",
     "xnyz_host_free", "xnyz_trim", "xnyz_compress", "xnyz_compress_device", "xnyz_decompress",
     "xnyz_decompress_device", "xnyz_free", "xnyz_stage_quantize", "xnyz_stage_recover", "xnyz_stage_hilbert",
-    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_sort_noalloc", "xnyz_decompress_into",
+    "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_fit_profile", "xnyz_compress_with_profile", "xnyz_sort_noalloc", "xnyz_decompress_into",
     "xnyz_batch_create", "xnyz_batch_destroy", "xnyz_batch_workers", "xnyz_batch_compress", "xnyz_batch_decompress",
     "xnyz_set_block_mode", "xnyz_set_model", "xnyz_model_param_count", "xnyz_last_block_info",
     "xnyz_batch_set_block_mode", "xnyz_stage_repos", "xnyz_block_features", "xnyz_block_search", "xnyz_block_cost",

@@ -19,6 +19,10 @@ contexts and streams on this rank's GPU), then appends the frames; nothing cross
 but the final statistics, so there is no device collective (the reference's mapreduce mode,
 which shuffles cells across ranks, is a different product and not built here).
 
+`--shared-codebook` (-normal only): rank 0 fits complete Huffman codebooks on block 0
+(fit_profile), broadcasts the profile, and every block is coded with it
+(compress_with_profile), so that all frames carry the same codebook bytes.
+
 `decompress` is the downstream tool the manifests are for: it rebuilds the point file with
 every block's decoded points at the block's input offset (points inside a block in
 container order, as the reference's decompressor returns them).
@@ -39,7 +43,10 @@ from dataclasses import dataclass, field
 import numpy as np
 
 POINT_BYTES = 12
-QUANTIZERS = {"cube": 0, "to": 1, "adaptive": 2}
+# Quantizer codes as the reference driver's compress_block picks them (mpi_driver.cpp:129-130):
+# "cube" is the cube quantizer and every other name, "adaptive" included, the truncated
+# octahedron.
+QUANTIZERS = {"cube": 0, "to": 1, "adaptive": 1}
 
 
 @dataclass
@@ -53,6 +60,7 @@ class Args:
     bound: float = 1e-3
     direct_threshold: int = 1024
     verify_roundtrip: bool = False
+    shared_codebook: bool = False
     window_bytes: int = 1 << 30  # host bytes of input per batch
     workers: int = 0
 
@@ -95,6 +103,7 @@ def parse_compress_args(argv) -> Args:
     a.mode = v.get("--mode", a.mode)
     a.direct_threshold = v.get("--direct-threshold", a.direct_threshold)
     a.verify_roundtrip = v.get("--verify-roundtrip", False)
+    a.shared_codebook = v.get("--shared-codebook", False)
     a.window_bytes = v.get("--window-bytes", a.window_bytes)
     a.workers = v.get("--workers", a.workers)
     if a.block_size <= 0 or a.block_size % POINT_BYTES:
@@ -107,8 +116,8 @@ def parse_compress_args(argv) -> Args:
         raise SystemExit("mapreduce mode (cross-rank cell shuffle) is not part of this driver")
     if a.mode not in ("-normal", "-rle"):
         raise SystemExit("--mode must be -normal or -rle")
-    if v.get("--shared-codebook"):
-        raise SystemExit("--shared-codebook (fit_profile / compress_with_profile) is not supported")
+    if a.shared_codebook and a.mode == "-rle":
+        raise SystemExit("--shared-codebook is not implemented for -rle mode")
     return a
 
 
@@ -165,6 +174,7 @@ class RankStats:
     comp_s: float = 0.0
     write_s: float = 0.0
     wall_s: float = 0.0
+    warmup_s: float = 0.0
     records: list = field(default_factory=list)
 
 
@@ -188,6 +198,13 @@ class _Dist:
     def barrier(self):
         if self.pg:
             self.pg.barrier()
+
+    def broadcast(self, obj, src: int = 0):
+        if not self.pg:
+            return obj
+        box = [obj]
+        self.pg.broadcast_object_list(box, src=src)
+        return box[0]
 
     def gather(self, obj):
         if not self.pg:
@@ -215,13 +232,40 @@ def _gpu_compressor(args: Args, device: int):
     return compress
 
 
-def _verify_block(args: Args, ctx, pts: np.ndarray, frame: bytes):
+def _gpu_fit_profile(args: Args, device: int, pts: np.ndarray) -> bytes:
+    """BlockCompressor::fit_profile on the warm-up block; the frame is dropped as there."""
+    import xnyzip_b200 as X
+    ctx = X.Context(device)
+    try:
+        _, prof = ctx.fit_profile(pts, QUANTIZERS[args.quantizer], float(np.float32(args.bound)), args.curve == "-h")
+    finally:
+        ctx.close()
+    return prof
+
+
+def _gpu_profile_compressor(args: Args, device: int, prof: bytes):
+    """compress_with_profile of each block (mpi_driver.cpp:123-142), one context."""
+    import xnyzip_b200 as X
+    ctx = X.Context(device)
+    q, l2, hil = QUANTIZERS[args.quantizer], float(np.float32(args.bound)), args.curve == "-h"
+
+    def compress(clouds):
+        return [ctx.compress_with_profile(c, q, l2, hil, prof) for c in clouds]
+
+    compress.close = ctx.close
+    return compress
+
+
+def _verify_block(args: Args, ctx, pts: np.ndarray, frame: bytes, profile: bytes | None = None):
     """--verify-roundtrip (mpi_driver.cpp:838-899): decompress the frame and check every point
     against the input in container order; -rle blocks are skipped as there."""
     q = QUANTIZERS[args.quantizer]
     l2 = float(np.float32(args.bound))
-    again, order = ctx.compress(pts, q, l2, args.curve == "-h", False, args.direct_threshold, use_zstd=True,
-                                want_order=True)
+    if profile is None:
+        again, order = ctx.compress(pts, q, l2, args.curve == "-h", False, args.direct_threshold, use_zstd=True,
+                                    want_order=True)
+    else:
+        again, order = ctx.compress_with_profile(pts, q, l2, args.curve == "-h", profile, want_order=True)
     if again != frame:
         raise RuntimeError("verify: recompressing the block gave different bytes")
     rec = ctx.decompress(frame, q, l2, False)
@@ -236,7 +280,9 @@ def _verify_block(args: Args, ctx, pts: np.ndarray, frame: bytes):
 
 def compress_file(args: Args, dist: _Dist, compressor=None, log=print) -> RankStats:
     """Runs the per-chunk compression of one rank.  `compressor(list of (n, 3) float32 arrays)
-    -> list of frames` defaults to the GPU batch path on this rank's device."""
+    -> list of frames` defaults to the GPU batch path on this rank's device; with
+    --shared-codebook a given compressor is called as compressor(None, block 0's points) ->
+    profile on rank 0 and as compressor(clouds, profile) -> frames."""
     os.makedirs(args.output_dir, exist_ok=True)
     file_size = os.path.getsize(args.input)
     aligned, num_blocks = block_layout(file_size, args.block_size)
@@ -248,7 +294,26 @@ def compress_file(args: Args, dist: _Dist, compressor=None, log=print) -> RankSt
         log(f"input={args.input} size={file_size} aligned={aligned} block_size={args.block_size} "
             f"num_blocks={num_blocks} nranks={nranks}")
     own = compressor is None
-    if own:
+    warmup_s = 0.0
+    prof = None
+    if args.shared_codebook:
+        # rank 0 fits the codebooks on block 0 and every rank codes every block with them
+        # (mpi_driver.cpp:722-781); a given `compressor(clouds, profile)` takes the profile
+        dist.barrier()
+        tw = time.perf_counter()
+        if rank == 0:
+            _, n0 = block_extent(0, args.block_size, aligned)
+            warm = np.fromfile(args.input, dtype=np.float32, count=n0 // 4).reshape(-1, 3)
+            prof = (_gpu_fit_profile(args, dist.local_rank, warm) if own else compressor(None, warm))
+            log(f"[shared-codebook] rank 0 fit profile: blob={len(prof)} bytes")
+        prof = dist.broadcast(prof, 0)
+        dist.barrier()
+        warmup_s = time.perf_counter() - tw
+        if own:
+            compressor = _gpu_profile_compressor(args, dist.local_rank, prof)
+        else:
+            compressor = (lambda clouds, _b=compressor, _p=prof: _b(clouds, _p))
+    elif own:
         compressor = _gpu_compressor(args, dist.local_rank)
     ctx = None
     if args.verify_roundtrip and args.mode == "-normal":
@@ -276,7 +341,7 @@ def compress_file(args: Args, dist: _Dist, compressor=None, log=print) -> RankSt
             frames = compressor(clouds)
             if ctx is not None:
                 for (b, _, _), pts, fr in zip(extents, clouds, frames):
-                    _verify_block(args, ctx, pts, fr)
+                    _verify_block(args, ctx, pts, fr, prof if args.shared_codebook else None)
             w = time.perf_counter()
             for (b, off, nbytes), fr in zip(extents, frames):
                 if fr is None:
@@ -297,6 +362,7 @@ def compress_file(args: Args, dist: _Dist, compressor=None, log=print) -> RankSt
                 f"out={st.compressed_bytes / 1e6:.2f}MB  rank_elapsed={e - t0:.2f}s")
     if own:
         compressor.close()
+    st.warmup_s = warmup_s
     if ctx is not None:
         ctx.close()
     dist.barrier()
@@ -309,7 +375,7 @@ def compress_file(args: Args, dist: _Dist, compressor=None, log=print) -> RankSt
 def _write_summary(args: Args, dist: _Dist, st: RankStats, num_blocks: int, log):
     """Totals and max-over-ranks phase times (mpi_driver.cpp:951-1036)."""
     mine = {k: getattr(st, k) for k in ("rank", "input_bytes", "compressed_bytes", "blocks", "read_s", "comp_s",
-                                         "write_s", "wall_s")}
+                                         "write_s", "wall_s", "warmup_s")}
     allr = dist.gather(mine)
     if dist.rank != 0:
         return
@@ -321,8 +387,8 @@ def _write_summary(args: Args, dist: _Dist, st: RankStats, num_blocks: int, log)
         "nranks": dist.size,
         "num_blocks": sum(r["blocks"] for r in allr),
         "block_size": args.block_size,
-        "shared_codebook": False,
-        "warmup_s": 0.0,
+        "shared_codebook": bool(args.shared_codebook),
+        "warmup_s": max(r["warmup_s"] for r in allr),
         "input_bytes": g_in,
         "compressed_bytes": g_out,
         "ratio": g_in / g_out if g_out else 0.0,

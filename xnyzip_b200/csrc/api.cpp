@@ -148,6 +148,10 @@ struct xnyz_ctx {
     std::map<std::string, std::pair<double, uint64_t>> host_ms;  // host phase wall time, calls
     // extended container (block parameters of the repos / SFC-delta stream)
     int block_mode = XNYZ_BLOCKS_OFF;
+    // shared codebooks (fit_profile / compress_with_profile): 0 off, 1 fit (complete
+    // codebooks, the profile of the call in share_out), 2 use share_rep / share_quad
+    int share_mode = 0;
+    std::vector<uint8_t> share_rep, share_quad, share_out;
     float* d_model = nullptr;      // predictor parameters (kParamCount FP32)
     float fallback_conf = 0.5f;    // learned mode: blocks below this confidence are searched
     xnyz_block_info last_blocks{};
@@ -650,7 +654,11 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     const int rx = S.max_cell[0], ry = S.max_cell[1], rz = S.max_cell[2];
     const bool defects = S.min_cell[2] < 0;  // truncated-octahedron cells at z = -1
     const int max_range = std::max({rx, ry, rz});
-    const bool direct = !cin && max_range < prm.direct_threshold;  // cell tables: always block mode
+    // cell tables and shared codebooks: always block mode (block_compressor.hpp:314-320)
+    const bool shared = c->share_mode != 0;
+    if (shared && (rle || cin || c->block_mode != XNYZ_BLOCKS_OFF))
+        return fail(XNYZ_ERR_INVALID_ARG, "shared codebooks code the -normal reference container only");
+    const bool direct = !cin && !shared && max_range < prm.direct_threshold;
 
     // ---- 2. key layout ----
     BlockKeyParams bkp{};
@@ -806,9 +814,25 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         if (!direct && H.hist_quad[s])
             st_quad.push_back(SymbolStat{static_cast<uint64_t>(s), H.hist_quad[s], H.first_quad[s]});
     }
-    const StreamCode code_rep = ext ? StreamCode{} : build_stream_code(SymType::U64, st_rep, U);
-    StreamCode code_quad;
-    if (!direct) code_quad = build_stream_code(SymType::U8, st_quad, U);
+    StreamCode code_rep, code_quad;
+    if (c->share_mode == 1) {  // fit_profile: codebooks covering every symbol 0..255
+        code_rep = build_complete_code(SymType::U64, st_rep, U, 255);
+        code_quad = build_complete_code(SymType::U8, st_quad, U, 255);
+        c->share_out.clear();
+        for (const auto* m : {&code_rep.meta, &code_quad.meta}) {  // serialize_profile layout
+            const uint32_t len = static_cast<uint32_t>(m->size());
+            for (int b = 0; b < 4; ++b) c->share_out.push_back(static_cast<uint8_t>(len >> (8 * b)));
+            c->share_out.insert(c->share_out.end(), m->begin(), m->end());
+        }
+    } else if (c->share_mode == 2) {  // compress_with_profile: the profile's codebooks
+        std::string e;
+        if (!loaded_stream_code(SymType::U64, c->share_rep.data(), c->share_rep.size(), st_rep, code_rep, e) ||
+            !loaded_stream_code(SymType::U8, c->share_quad.data(), c->share_quad.size(), st_quad, code_quad, e))
+            return fail(XNYZ_ERR_INVALID_ARG, "profile: " + e);
+    } else {
+        if (!ext) code_rep = build_stream_code(SymType::U64, st_rep, U);
+        if (!direct) code_quad = build_stream_code(SymType::U8, st_quad, U);
+    }
     StreamCode code_cnt;
     std::vector<uint32_t> sparse_val, sparse_bits;
     std::vector<uint8_t> sparse_len;
@@ -1779,6 +1803,63 @@ xnyz_status xnyz_compress(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_
         *info = R.info;
     }
     return XNYZ_OK;
+}
+
+namespace {
+// Sets the context's shared-codebook mode for one call and clears it afterwards.
+struct ShareScope {
+    xnyz_ctx* c;
+    ShareScope(xnyz_ctx* cc, int mode) : c(cc) { c->share_mode = mode; }
+    ~ShareScope() {
+        c->share_mode = 0;
+        c->share_rep.clear();
+        c->share_quad.clear();
+    }
+};
+
+// deserialize_profile (composer/block_encoding_profile.hpp:51-72), strict about sizes.
+bool parse_profile(const uint8_t* p, uint64_t len, std::vector<uint8_t>& rep, std::vector<uint8_t>& quad) {
+    uint64_t pos = 0;
+    for (auto* dst : {&rep, &quad}) {
+        if (pos + 4 > len) return false;
+        const uint32_t n = uint32_t(p[pos]) | (uint32_t(p[pos + 1]) << 8) | (uint32_t(p[pos + 2]) << 16) |
+                           (uint32_t(p[pos + 3]) << 24);
+        pos += 4;
+        if (n > len - pos) return false;
+        dst->assign(p + pos, p + pos + n);
+        pos += n;
+    }
+    return true;
+}
+}  // namespace
+
+xnyz_status xnyz_fit_profile(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_device, const xnyz_params* params,
+                             int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order, uint8_t** profile,
+                             uint64_t* profile_len) {
+    clear_stale_cuda_error();
+    if (!c || !params || !profile || !profile_len) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    *profile = nullptr;
+    *profile_len = 0;
+    ShareScope scope(c, 1);
+    TRY(xnyz_compress(c, xyz, n, xyz_is_device, params, use_zstd, out, out_len, sort_order, nullptr));
+    uint8_t* p = static_cast<uint8_t*>(std::malloc(c->share_out.size()));
+    if (!p) return fail(XNYZ_ERR_OOM, "host allocation");
+    std::memcpy(p, c->share_out.data(), c->share_out.size());
+    *profile = p;
+    *profile_len = c->share_out.size();
+    return XNYZ_OK;
+}
+
+xnyz_status xnyz_compress_with_profile(xnyz_ctx* c, const float* xyz, uint64_t n, int xyz_is_device,
+                                       const xnyz_params* params, const uint8_t* profile, uint64_t profile_len,
+                                       int use_zstd, uint8_t** out, uint64_t* out_len, uint64_t* sort_order) {
+    clear_stale_cuda_error();
+    if (!c || !params || (!profile && profile_len)) return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    ShareScope scope(c, 2);
+    if (!profile || !parse_profile(profile, profile_len, c->share_rep, c->share_quad) || c->share_rep.empty() ||
+        c->share_quad.empty())
+        return fail(XNYZ_ERR_INVALID_ARG, "compress_with_profile: empty or malformed profile");
+    return xnyz_compress(c, xyz, n, xyz_is_device, params, use_zstd, out, out_len, sort_order, nullptr);
 }
 
 xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, const xnyz_params* params,

@@ -67,6 +67,66 @@ public:
         from_freq(freq);
     }
 
+    // build_complete (:70-85): fresh freq map, then the missing values of [0, amax].
+    void build_complete(const std::vector<std::pair<T, uint64_t>>& ordered, T amax) {
+        code_table.clear();
+        use_eg = false;
+        eg_k = 0;
+        std::unordered_map<T, uint64_t> freq;
+        for (const auto& sc : ordered) freq[sc.first] = sc.second;
+        for (T s = 0; s <= amax; ++s) {
+            if (freq.find(s) == freq.end()) freq[s] = 1;
+            if (s == std::numeric_limits<T>::max()) break;
+        }
+        from_freq(freq);
+    }
+
+    // load_meta (:172-203) on a fresh encoder: entries inserted in the meta's order (a
+    // repeated symbol keeps its last code).
+    bool load(const uint8_t* m, uint64_t len, std::string& err) {
+        code_table.clear();
+        use_eg = false;
+        eg_k = 0;
+        uint64_t p = 0;
+        if (len >= 4 && m[0] == 0xE1 && m[1] == 0xC1 && m[2] == 0x01) {
+            p = 4;
+            if (m[3] == 0x01) {
+                eg_k = len > 4 ? m[4] : 0;
+                use_eg = true;
+                return true;
+            }
+        }
+        if (p + 4 > len) {
+            err = "truncated Huffman meta in the profile";
+            return false;
+        }
+        const uint32_t count =
+            (uint32_t(m[p]) << 24) | (uint32_t(m[p + 1]) << 16) | (uint32_t(m[p + 2]) << 8) | uint32_t(m[p + 3]);
+        p += 4;
+        const uint64_t entry = sizeof(T) + 1 + 4;
+        if (count > (len - p) / entry) {
+            err = "truncated Huffman meta in the profile";
+            return false;
+        }
+        for (uint32_t i = 0; i < count; ++i) {
+            T sym;
+            if constexpr (sizeof(T) == 8) {
+                uint64_t v = 0;
+                for (int k = 0; k < 8; ++k) v = (v << 8) | m[p++];
+                sym = static_cast<T>(v);
+            } else {
+                std::memcpy(&sym, m + p, sizeof(T));
+                p += sizeof(T);
+            }
+            const uint8_t l = m[p++];
+            const uint32_t b =
+                (uint32_t(m[p]) << 24) | (uint32_t(m[p + 1]) << 16) | (uint32_t(m[p + 2]) << 8) | uint32_t(m[p + 3]);
+            p += 4;
+            code_table[sym] = Code{b, l};
+        }
+        return true;
+    }
+
     std::vector<uint8_t> meta() const {
         if (use_eg) return {0xE1, 0xC1, 0x01, 0x01, eg_k};
         std::vector<uint8_t> out;
@@ -265,6 +325,56 @@ StreamCode build_stream_code(SymType type, std::vector<SymbolStat> stats, uint64
         case SymType::U64: return build_one<uint64_t>(stats, total);
         case SymType::U8: return build_one<uint8_t>(stats, total);
         default: return build_one<int>(stats, total);
+    }
+}
+
+StreamCode build_complete_code(SymType type, std::vector<SymbolStat> stats, uint64_t total, uint64_t alphabet_max) {
+    (void)total;
+    switch (type) {
+        case SymType::U64: {
+            auto ordered = ordered_stats<uint64_t>(stats);
+            Replay<uint64_t> r;
+            r.build_complete(ordered, alphabet_max);
+            return finish(r, ordered);
+        }
+        case SymType::U8: {
+            auto ordered = ordered_stats<uint8_t>(stats);
+            Replay<uint8_t> r;
+            r.build_complete(ordered, static_cast<uint8_t>(std::min<uint64_t>(alphabet_max, 255)));
+            return finish(r, ordered);
+        }
+        default: {
+            auto ordered = ordered_stats<int>(stats);
+            Replay<int> r;
+            r.build_complete(ordered, static_cast<int>(std::min<uint64_t>(alphabet_max, 0x7fffffff)));
+            return finish(r, ordered);
+        }
+    }
+}
+
+namespace {
+template <typename T>
+bool loaded_one(const uint8_t* meta, uint64_t len, std::vector<SymbolStat>& stats, StreamCode& out, std::string& err) {
+    auto ordered = ordered_stats<T>(stats);
+    Replay<T> r;
+    if (!r.load(meta, len, err)) return false;
+    if (!r.use_eg)
+        for (const auto& sc : ordered)
+            if (!r.code_table.count(sc.first)) {
+                err = "a symbol of the stream has no code in the profile";
+                return false;
+            }
+    out = finish(r, ordered);
+    return true;
+}
+}  // namespace
+
+bool loaded_stream_code(SymType type, const uint8_t* meta, uint64_t len, std::vector<SymbolStat> stats,
+                        StreamCode& out, std::string& err) {
+    switch (type) {
+        case SymType::U64: return loaded_one<uint64_t>(meta, len, stats, out, err);
+        case SymType::U8: return loaded_one<uint8_t>(meta, len, stats, out, err);
+        default: return loaded_one<int>(meta, len, stats, out, err);
     }
 }
 

@@ -47,6 +47,17 @@ StreamCode build_stream_code(SymType type, std::vector<SymbolStat> stats, uint64
 // to exp-Golomb when the meta exceeds a quarter of the data, build again on the same object.
 StreamCode build_count_code(std::vector<SymbolStat> stats, uint64_t total);
 
+// HuffmanEncoder<T>::build_complete (huffman_encoder.hpp:70-85), the shared-codebook fit:
+// the data's symbols in first-occurrence order, then every value of [0, alphabet_max] the data
+// lacks with frequency 1, built without the exp-Golomb switch.
+StreamCode build_complete_code(SymType type, std::vector<SymbolStat> stats, uint64_t total, uint64_t alphabet_max);
+
+// A fresh HuffmanEncoder<T> given `meta` by load_meta (huffman_encoder.hpp:172-203), then
+// get_meta + encode: the meta written back lists the loaded table in its own iteration
+// order.  Fails when the meta is malformed or a symbol of `stats` has no code.
+bool loaded_stream_code(SymType type, const uint8_t* meta, uint64_t len, std::vector<SymbolStat> stats,
+                        StreamCode& out, std::string& err);
+
 // Parsed meta of a stream for decoding (load_meta, huffman_encoder.hpp:172-203).
 struct ParsedMeta {
     bool exp_golomb = false;
