@@ -8,7 +8,9 @@ copies), Hilbert curve, -rle container, both quantizers (to, cube) x L2 bounds
 
   value : compress+decompress GB/s (12 bytes per input point) with the points resident in
           HBM, the pre-zstd container produced and consumed in HBM (xnyz_compress_device /
-          xnyz_decompress_device), device time from CUDA events on the library's stream.
+          xnyz_decompress_device), device time from CUDA events on the library's stream; the
+          variants, which are independent, run on --pipes contexts (streams) from host threads
+          so that one variant's kernels fill another's gaps.
   e2e   : the same through the host-buffer C ABI, batched (xnyz_batch_compress /
           xnyz_batch_decompress: worker threads with one context each): pinned host points
           in, the reference's zstd level-3 frames out (libzstd 1.5.7 on the host), frames in,
@@ -197,15 +199,58 @@ def run_gpu(args):
     max_over_ranks = sync.max
 
     # ---- device-resident step ----
-    def device_step():
-        containers = []
-        for q, l2, hil, rle in variants:
-            p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
-            containers.append(ln)
-            _, nout = ctx.decompress_device(p, ln, q, l2, rle)
+    def run_variants(c, vs):
+        lens = []
+        for q, l2, hil, rle in vs:
+            p, ln = c.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
+            lens.append(ln)
+            _, nout = c.decompress_device(p, ln, q, l2, rle)
             if nout != n:
                 raise RuntimeError(f"decoded {nout} points, expected {n}")
-        return containers
+        return lens
+
+    def serial_step():  # every variant on the one context (the profiled step)
+        return run_variants(ctx, variants)
+
+    # The timed step runs the variants, which are independent, on `pipes` contexts with their
+    # own streams from host threads, so that one variant's kernels fill the gaps of another's
+    # (its host-side codebook work, latency-bound decoders).  The other streams wait for an
+    # event on the main stream before their first call and the main stream waits for theirs
+    # at the end: the CUDA events on the main stream bracket all of the step's work.
+    pipes = max(1, min(args.pipes, len(variants)))
+    pipe_streams = [stream] + [torch.cuda.Stream(dev) for _ in range(pipes - 1)]
+    pipe_ctx = [ctx] + [X.Context(local, stream=s.cuda_stream) for s in pipe_streams[1:]]
+
+    def device_step():
+        if pipes == 1:
+            return serial_step()
+        start = torch.cuda.Event()
+        start.record(stream)
+        for s in pipe_streams[1:]:
+            s.wait_event(start)
+        out, errs = [None] * pipes, []
+
+        def worker(k):
+            try:
+                out[k] = run_variants(pipe_ctx[k], variants[k::pipes])
+            except Exception as e:  # re-raised on the main thread
+                errs.append(e)
+
+        ths = [threading.Thread(target=worker, args=(k,)) for k in range(pipes)]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        if errs:
+            raise errs[0]
+        for s in pipe_streams[1:]:
+            done = torch.cuda.Event()
+            done.record(s)
+            stream.wait_event(done)
+        lens = [0] * len(variants)
+        for k in range(pipes):
+            lens[k::pipes] = out[k]
+        return lens
 
     for _ in range(args.warmup):
         clens = device_step()
@@ -226,8 +271,10 @@ def run_gpu(args):
     barrier()
     # one more step with per-stage CUDA events, the side streams' work issued on the context's
     # stream (xnyz_profile mode 2), so that each stage's time is its own: the roofline
+    for c in pipe_ctx[1:]:  # their workspaces are not needed past the timed step
+        c.close()
     ctx.profile(2)
-    device_step()
+    serial_step()
     prof_all = ctx.profile_read()
     ctx.profile(False)
     prof = {k: v for k, v in prof_all.items() if not k.startswith("host:")}
@@ -338,7 +385,8 @@ def run_gpu(args):
                 "variants": [vname(v) for v in variants],
                 "direct_threshold": 1024,
                 "l2_flush": f"inputs ({12 * n / 1e6:.0f} MB per cloud) exceed the 126 MB L2",
-                "value_path": "device-resident points and pre-zstd container",
+                "value_path": f"device-resident points and pre-zstd container; the independent variants spread "
+                              f"over {pipes} contexts / streams, CUDA events on the main stream bracketing all",
                 "e2e_path": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
                             "xnyz_batch_compress / xnyz_batch_decompress",
                 "parallelism": f"replicas x{world}",
@@ -604,6 +652,7 @@ def main():
     ap.add_argument("--workload", default="terrain", choices=sorted(WORKLOADS))
     ap.add_argument("--points", type=int, default=0, help="points of the cloud (0: the workload's size)")
     ap.add_argument("--variants", type=int, default=6)
+    ap.add_argument("--pipes", type=int, default=3, help="contexts (streams) the timed step spreads the variants over")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-points", type=int, default=1_000_000)
     ap.add_argument("--chunk", type=int, default=150_000, help="points per chunk (e2e and the reference arm)")

@@ -14,8 +14,8 @@
 // decodes warp-parallel (escape j's unary part lies between the (j-1)-th and j-th zero of U).
 //
 // Kernels (one warp per block): features for the parameter predictor, the exhaustive search
-// over all 33 x 32 (w, k) pairs (training labels, fallback and judge), the cost of given
-// pairs, the encoder and the decoder.
+// over all 33 x 32 (w, k) pairs (training labels, fallback and the yardstick of the size
+// penalty), the cost of given pairs, the encoder and the decoder.
 #include "device_common.cuh"
 #include "kernels.h"
 

@@ -258,7 +258,7 @@ struct RecoverArgs {
 // Warp w owns units [512 w, 512 w + 512) of the tile and takes them 32 at a time, one per
 // lane: staged symbols are read without bank conflicts, patches, counts and block starts
 // are read coalesced, and the points of a round are written to consecutive addresses.
-// Round 1 folds each warp's zero symbols, counts and quad / block segments, round 2 its
+// Pass 1 folds each warp's zero symbols, counts and quad / block segments, pass 2 its
 // repos segments (or SFC sums); the block combines the warps, chained scans combine the
 // tiles, and the final pass rebuilds every running value with warp scans from its warp's
 // starting carry.
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         return 0;
     };
 
-    // ---- round 1: zero symbols, counts, quad and block segments per warp ----
+    // ---- pass 1: zero symbols, counts, quad and block segments per warp ----
     {
         u64 z = 0, c = 0, bc = 0;
         u32 qc = 0;
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     if (!rle && tid == 0) base_count = 0;
     __syncthreads();
 
-    // ---- round 2: repos segments (block mode) or SFC sums (direct mode) per warp ----
+    // ---- pass 2: repos segments (block mode) or SFC sums (direct mode) per warp ----
     {
         u64 zc = base_zero + wz[w];
         u64 d = 0, rc = 0;
