@@ -141,6 +141,19 @@ def make_cloud(workload: str, n: int, seed: int):
     return S.terrain(n, seed)
 
 
+def workload_config(workload: str, n: int, variants) -> dict:
+    """The workload part of the bench line's config, the same for both arms."""
+    return {
+        "workload": (f"terrain {n} points, Hilbert, -rle, quantizers to/cube x L2 {{0.001,0.01,0.1}}"
+                     if workload == "terrain" else
+                     f"spheres {n} points on 200,000 spheres, TO, L2 0.5, Morton, -normal and -rle")
+                    + f"; one step = compress+decompress of all {len(variants)} variants",
+        "points": n,
+        "variants": [vname(v) for v in variants],
+        "direct_threshold": 1024,
+    }
+
+
 class RankSync:
     """Barrier and max-over-ranks of a timing: one value per rank, the job's time is the
     slowest rank's.  NCCL with a device tensor on GPUs, gloo with a host tensor elsewhere."""
@@ -377,13 +390,7 @@ def run_gpu(args):
             "data": (f"synthetic {'terrain-LiDAR' if args.workload == 'terrain' else 'clustered-surface'} "
                      f"stand-in (seeded, {n} points), generated on the host"),
             "config": {
-                "workload": (f"terrain {n} points, Hilbert, -rle, quantizers to/cube x L2 {{0.001,0.01,0.1}}"
-                             if args.workload == "terrain" else
-                             f"spheres {n} points on 200,000 spheres, TO, L2 0.5, Morton, -normal and -rle")
-                            + f"; one step = compress+decompress of all {len(variants)} variants",
-                "points": n,
-                "variants": [vname(v) for v in variants],
-                "direct_threshold": 1024,
+                **workload_config(args.workload, n, variants),
                 "l2_flush": f"inputs ({12 * n / 1e6:.0f} MB per cloud) exceed the 126 MB L2",
                 "value_path": f"device-resident points and pre-zstd container; the independent variants spread "
                               f"over {pipes} contexts / streams, CUDA events on the main stream bracketing all",
@@ -637,7 +644,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}, {len(variants)} variants; host CPU reference", "points": n_total},
+        "config": {**workload_config(args.workload, args.points or WORKLOADS[args.workload][1], variants),
+                   "sample_points_per_step": n_total,
+                   "parallelism": f"{threads} host threads, one {chunk}-point chunk each (per-chunk mode)"},
         "cpu_baseline": {"value": round(value, 5), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 5), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
