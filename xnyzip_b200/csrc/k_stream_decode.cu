@@ -27,10 +27,13 @@ namespace dev {
 namespace {
 
 constexpr int T = kDecodeBlockSubs;     // subsequences (threads) per block
-constexpr int S = kDecodeSubBits;       // bits per subsequence
-constexpr int BLOCK_WORDS = T * S / 32; // stream words per block
 constexpr int HALO = 8;                 // words staged after the block's range
-constexpr int STAGED = BLOCK_WORDS + HALO;
+// Subsequence geometry per code: bits per subsequence, staged words per block.
+template <int KIND>
+struct Geo {
+    static constexpr int S = KIND == kCodeGolombRice ? kDecodeSubBitsGR : kDecodeSubBits;
+    static constexpr int STAGED = T * S / 32 + HALO;
+};
 constexpr int WIN = 256;                // root bitmaps cover codeword starts in [0, WIN)
 constexpr int WINW = WIN / 32;
 constexpr int R = 3;                    // recorded root chains per subsequence
@@ -38,7 +41,9 @@ constexpr int kMaxL = kDecodeMaxL;
 constexpr int kMaxRootBits = 11;
 constexpr u32 kOOD = 0xffu;             // exit outside the next subsequence's entry range
 constexpr u64 kFar = 1ull << 20;        // length given to an invalid Huffman code: ends the chain
-static_assert(S % 32 == 0 && T % 32 == 0 && T <= 1024 && WIN <= S, "decode geometry");
+static_assert(kDecodeSubBits % 32 == 0 && kDecodeSubBitsGR % 32 == 0 && T % 32 == 0 && T <= 1024 &&
+                  WIN <= kDecodeSubBits && WIN <= kDecodeSubBitsGR && kDecodeSubBits <= kDecodeSubBitsGR,
+              "decode geometry");
 
 // ------------------------------------------------------------- stream source ----------
 // A stream starts `base` (< 32) bits into `g`.  Word k of `g` is read from shared memory
@@ -50,9 +55,10 @@ struct Src {
     u64 nwords;
     const u32* sm;
     u64 sm_w0;
+    u64 staged;  // words in sm
     __device__ __forceinline__ u32 word(u64 k) const {
         const u64 d = k - sm_w0;
-        if (d < (u64)STAGED) return sm[d];
+        if (d < staged) return sm[d];
         return k < nwords ? __ldg(g + k) : 0u;
     }
     __device__ __forceinline__ u32 word_be(u64 k) const { return __byte_perm(word(k), 0, 0x0123); }
@@ -329,6 +335,7 @@ __device__ __forceinline__ u64 entry_offset(const Src& s, u32 i, u64 Bsub, int k
 // Returns false (table incomplete) when a codeword is too long for the masks or the stream
 // ends within reach; the caller then runs the generic loop.
 __device__ bool gr_lockstep_table(const Src& src, u64 B, u64 Bend, int k, u32* tab, int t, bool valid) {
+    constexpr int S = Geo<kCodeGolombRice>::S;
     const u32 span = valid ? (u32)(Bend - B) : 0u;
     const bool full = span == (u32)S;
     // near the end of the stream codewords may run past it (the generic decoder gives those
@@ -450,8 +457,10 @@ struct Args {
 };
 
 // Shared memory: scount[T] u64 | sw[STAGED] | bm[R][WINW][T] | sstart[T] | slot | tab[L][T] | root[2^rb]
-constexpr size_t kFixedSmem = 8 * T + 4 * (STAGED + R * WINW * T + T + 4);
-__host__ __device__ constexpr size_t smem_for(int L, int rb) { return kFixedSmem + 4ull * L * T + (rb ? 4ull << rb : 0); }
+template <int KIND>
+__host__ __device__ constexpr size_t smem_for(int L, int rb) {
+    return 8 * T + 4 * (Geo<KIND>::STAGED + R * WINW * T + T + 4) + 4ull * L * T + (rb ? 4ull << rb : 0);
+}
 
 // Output of symbols: u8 streams pack four symbols per 32-bit store where a word lies inside
 // the thread's range.
@@ -481,6 +490,8 @@ struct ByteOut {
 
 template <int KIND>
 __global__ void __launch_bounds__(T) decode_stream_kernel(Args a) {
+    constexpr int S = Geo<KIND>::S;
+    constexpr int STAGED = Geo<KIND>::STAGED;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64* scount = reinterpret_cast<u64*>(smem_raw);
     u32* sw = reinterpret_cast<u32*>(scount + T);
@@ -504,6 +515,7 @@ __global__ void __launch_bounds__(T) decode_stream_kernel(Args a) {
     src.nwords = (a.base + a.total_bits + 31) >> 5;
     src.sm = sw;
     src.sm_w0 = first_sub * (S / 32);
+    src.staged = STAGED;
     for (int i = t; i < STAGED; i += T) {
         const u64 k = src.sm_w0 + i;
         sw[i] = k < src.nwords ? __ldg(a.words + k) : 0u;
@@ -838,7 +850,8 @@ __global__ void decode_sequential_kernel(Args a) {
     src.total_bits = a.total_bits;
     src.nwords = (a.base + a.total_bits + 31) >> 5;
     src.sm = nullptr;
-    src.sm_w0 = ~0ull >> 1;  // nothing staged
+    src.sm_w0 = 0;
+    src.staged = 0;  // nothing staged
     Code code = a.code;
     code.root = a.root_global;
     u64 p = 0, i = 0;
@@ -869,6 +882,7 @@ Args make_args(int kind, const uint32_t* words, uint64_t base_bits, uint64_t tot
     a.words = words;
     a.base = (u32)base_bits;
     a.total_bits = total_bits;
+    const u64 S = kind == kCodeGolombRice ? (u64)kDecodeSubBitsGR : (u64)kDecodeSubBits;
     a.nsub = (total_bits + S - 1) / S;
     a.L = kind == kCodeGolombRice ? (t.param + 2 < kMaxL ? t.param + 2 : kMaxL) : (L < 1 ? 1 : (L > kMaxL ? kMaxL : L));
     a.code.root = t.root;
@@ -908,8 +922,10 @@ void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, u
     // The launch uses what this stream needs; the function's limit is always set to the
     // largest size any stream can need (the same value from every thread, so concurrent
     // launches from other contexts cannot lower it between this call and the launch).
-    const int smem = (int)smem_for(a.L, a.code.rb);
-    const int smem_max = (int)smem_for(kMaxL, kMaxRootBits);
+    const int smem = kind == kCodeGolombRice ? (int)smem_for<kCodeGolombRice>(a.L, a.code.rb)
+                                             : (int)smem_for<kCodeHuffman>(a.L, a.code.rb);
+    const int smem_max = kind == kCodeGolombRice ? (int)smem_for<kCodeGolombRice>(kMaxL, kMaxRootBits)
+                                                 : (int)smem_for<kCodeHuffman>(kMaxL, kMaxRootBits);
     if (kind == kCodeHuffman) {
         cudaFuncSetAttribute(decode_stream_kernel<kCodeHuffman>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
         decode_stream_kernel<kCodeHuffman><<<tiles, T, smem, st>>>(a);

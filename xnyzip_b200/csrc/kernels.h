@@ -190,10 +190,12 @@ struct DecodeTable {
     int zigzag;  // exp-Golomb of a signed symbol type
 };
 constexpr int kDecodeMaxL = 64;       // longest entry offset tracked per subsequence
-constexpr int kDecodeSubBits = 512;   // bits per subsequence (thread)
+constexpr int kDecodeSubBits = 512;   // bits per subsequence (thread): Huffman, exp-Golomb
+constexpr int kDecodeSubBitsGR = 1024;  // Golomb-Rice (longer subsequences amortise its entry tables)
 constexpr int kDecodeBlockSubs = 128; // subsequences per thread block
 // flag: [tiles]; agg: [tiles * kDecodeMaxL]; inc: [tiles * 2];
-// tiles = ceil(ceil(bits / kDecodeSubBits) / kDecodeBlockSubs).
+// tiles = ceil(ceil(bits / sub bits) / kDecodeBlockSubs) (kDecodeSubBits, the smaller, bounds
+// the tiles of every kind).
 // The stream starts `base_bits` (< 32) into `words`.  L = entry offsets tracked (the longest
 // codeword; Golomb-Rice derives k + 2 from its parameter, L_run is unused).
 void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t,
