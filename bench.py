@@ -506,7 +506,7 @@ def batched_measure(ctx, stream, dev, count, workers):
     plain: one context, per-cloud compress_device + decompress_device in order.  batched:
     xnyz_batch_roundtrip_device with worker streams per size class chosen by
     xnyz_batch_autotune; with the reference container and with learned block parameters.
-    Device-synchronised wall clock (the work of one step spans many streams)."""
+    Device-synchronised wall clock (the work of one step spans many streams), best of 3."""
     import torch
     import xnyzip_b200 as X
     from xnyzip_b200 import synthetic_gpu as G
@@ -526,17 +526,24 @@ def batched_measure(ctx, stream, dev, count, workers):
             if nout != n:
                 raise RuntimeError("plain round trip lost points")
 
-    def timed(fn, reps=2):
+    rep_s = {}
+
+    def timed(fn, name, reps=3):
+        """Best of `reps` timed runs after one warm-up (a run that grows a worker's workspace
+        or loads its predictor pays cudaMalloc's device synchronisation)."""
         fn()
-        torch.cuda.synchronize(dev)
-        t = time.perf_counter()
+        ts = []
         for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
             fn()
-        torch.cuda.synchronize(dev)
-        return (time.perf_counter() - t) / reps
+            torch.cuda.synchronize(dev)
+            ts.append(time.perf_counter() - t)
+        rep_s[name] = [round(x, 4) for x in ts]
+        return min(ts)
 
     ctx.set_block_mode(0)
-    t_plain = timed(plain_step)
+    t_plain = timed(plain_step, "plain")
     batch = X.Batch(0, workers)
     out = {"clouds": count, "points": int(total), "generate_s": round(gen_s, 2)}
     res = {"plain": t_plain}
@@ -550,10 +557,11 @@ def batched_measure(ctx, stream, dev, count, workers):
                 raise RuntimeError("batched round trip lost points")
             return ln
 
-        res[name] = timed(bstep)
+        res[name] = timed(bstep, name)
         out[f"{name}_workers_per_class"] = tune
         out[f"{name}_bits_per_point_prezstd"] = round(8.0 * float(bstep().sum()) / total, 4)
     batch.close()
+    out["rep_s"] = rep_s
     out["points_per_s"] = {k: round(total / v, 1) for k, v in res.items()}
     out["GB_s"] = {k: round(12.0 * total / v / 1e9, 3) for k, v in res.items()}
     out["speedup_vs_plain"] = {k: round(res["plain"] / v, 3) for k, v in res.items() if k != "plain"}
