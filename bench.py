@@ -314,14 +314,22 @@ def run_gpu(args):
     chunk_bytes = {}
 
     def e2e_chunked_step():
-        frames = batch.compress(c_clouds, c_params, as_bytes=False)
-        ns = batch.decompress(frames, c_dparams, c_outs)
-        if ns != [b - a for _ in variants for (a, b) in bounds]:
-            raise RuntimeError("e2e (chunked) decode size mismatch")
+        if args.e2e_mode == "roundtrip":  # each chunk's compress + decompress on one worker
+            frames = batch.roundtrip(c_clouds, c_params, c_outs)
+        else:  # every compress, then every decompress
+            frames = batch.compress(c_clouds, c_params, as_bytes=False)
+            ns = batch.decompress(frames, c_dparams, c_outs)
+            if ns != [b - a for _ in variants for (a, b) in bounds]:
+                raise RuntimeError("e2e (chunked) decode size mismatch")
         for vi, v in enumerate(variants):
             chunk_bytes[v] = sum(len(f) for f in frames[vi * len(bounds):(vi + 1) * len(bounds)])
 
     def e2e_monolithic_step():
+        if args.e2e_mode == "roundtrip":
+            frames = batch.roundtrip(m_clouds, m_params, outs)
+            for v, f in zip(variants, frames):
+                frame_bytes[v] = len(f)
+            return
         frames = batch.compress(m_clouds, m_params, as_bytes=False)
         ns = batch.decompress(frames, m_dparams, outs)
         if ns != [n] * len(variants):
@@ -395,7 +403,8 @@ def run_gpu(args):
                 "value_path": f"device-resident points and pre-zstd container; the independent variants spread "
                               f"over {pipes} contexts / streams, CUDA events on the main stream bracketing all",
                 "e2e_path": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
-                            "xnyz_batch_compress / xnyz_batch_decompress",
+                            + ("xnyz_batch_roundtrip (each chunk's pair on one worker)" if args.e2e_mode == "roundtrip"
+                               else "xnyz_batch_compress then xnyz_batch_decompress"),
                 "parallelism": f"replicas x{world}",
             },
             "bits_per_point": bpp,
@@ -669,6 +678,9 @@ def main():
     ap.add_argument("--workload", default="terrain", choices=sorted(WORKLOADS))
     ap.add_argument("--points", type=int, default=0, help="points of the cloud (0: the workload's size)")
     ap.add_argument("--variants", type=int, default=6)
+    ap.add_argument("--e2e-mode", default="roundtrip", choices=["roundtrip", "phases"],
+                    help="e2e: xnyz_batch_roundtrip (each chunk compressed and decompressed on one worker) or "
+                         "xnyz_batch_compress then xnyz_batch_decompress")
     ap.add_argument("--pipes", type=int, default=3, help="contexts (streams) the timed step spreads the variants over")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-points", type=int, default=1_000_000)

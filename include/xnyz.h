@@ -197,6 +197,15 @@ xnyz_status xnyz_batch_decompress(xnyz_batch* batch, uint64_t count, const uint8
                                   int is_zstd, const int* quantizer, const float* l2_bound, const int* rle,
                                   float* const* xyz, const uint64_t* capacity, uint64_t* n, xnyz_status* item_status);
 
+/* No counterpart in the reference.  Host-buffer round trip of every cloud: the zstd frame
+ * (malloc'd in frame[i], free with xnyz_free; byte-identical to xnyz_compress) and its
+ * decompression into out[i] (n[i] points, in container order as xnyz_decompress returns
+ * them), both on the same worker, so that one cloud's host zstd work overlaps another's GPU
+ * work.  The reference's per-chunk threads do the same pair per chunk. */
+xnyz_status xnyz_batch_roundtrip(xnyz_batch* batch, uint64_t count, const float* const* xyz, const uint64_t* n,
+                                 const xnyz_params* params, uint8_t** frame, uint64_t* frame_len, float* const* out,
+                                 xnyz_status* item_status);
+
 /* ---- distributed-RLE cell tables ------------------------------------------------------------ */
 
 /* XnYZip::BlockCompressorRLE<float>::encode_cells_with_counts (composer/block_compressor_rle.hpp:341-470):

@@ -40,6 +40,22 @@ def test_batch_matches_single_calls(ctx, xnyz, workers):
         b.close()
 
 
+@pytest.mark.parametrize("workers", [1, 4])
+def test_batch_host_roundtrip_matches_single_calls(ctx, xnyz, workers):
+    """xnyz_batch_roundtrip: the frames of xnyz_compress and the points of xnyz_decompress."""
+    clouds, params = _clouds()
+    b = xnyz.Batch(0, workers)
+    try:
+        outs = [np.full((x.shape[0], 3), np.nan, np.float32) for x in clouds]
+        frames = b.roundtrip(clouds, params, outs, as_bytes=True)
+        for x, p, f, o in zip(clouds, params, frames, outs):
+            assert f == ctx.compress(x, p[0], p[1], p[2], p[3], p[4])
+            ref = ctx.decompress(f, p[0], p[1], p[3])
+            assert np.array_equal(o.view(np.uint32), ref.view(np.uint32))
+    finally:
+        b.close()
+
+
 def test_batch_reports_failing_item(xnyz):
     clouds, params = _clouds()
     params = list(params)

@@ -310,6 +310,39 @@ class Batch:
         N.check(s)
         return frames
 
+    def roundtrip(self, clouds, params, outs, as_bytes: bool = False):
+        """xnyz_batch_roundtrip: every cloud compressed to its zstd frame and decompressed into
+        outs[i] on the same worker.  params: (quantizer, l2, hilbert, rle[, direct_threshold]);
+        outs: C-contiguous float32 arrays of n_i points.  Returns the frames (uint8 arrays over
+        the library's buffers, or bytes)."""
+        k = len(clouds)
+        arrs = [np.ascontiguousarray(c, dtype=np.float32).reshape(-1, 3) for c in clouds]
+        os_ = [o.reshape(-1, 3) for o in outs]
+        for a, o in zip(arrs, os_):
+            if o.dtype != np.float32 or not o.flags.c_contiguous or o.shape[0] < a.shape[0]:
+                raise ValueError("outputs must be C-contiguous float32 arrays of n points")
+        ptrs = (C.c_void_p * k)(*[a.ctypes.data for a in arrs])
+        ns = (C.c_uint64 * k)(*[a.shape[0] for a in arrs])
+        prm = (Params * k)(*[Params(int(p[0]), float(p[1]), int(bool(p[2])), int(bool(p[3])),
+                                    int(p[4]) if len(p) > 4 else 1024) for p in params])
+        frames_p = (C.c_void_p * k)()
+        lens = (C.c_uint64 * k)()
+        optr = (C.c_void_p * k)(*[o.ctypes.data for o in os_])
+        s = N.batch_roundtrip(self.handle, k, ptrs, ns, prm, frames_p, lens, optr, None)
+        frames = []
+        for i in range(k):
+            if not frames_p[i]:
+                frames.append(None)
+            elif as_bytes:
+                frames.append(C.string_at(frames_p[i], lens[i]))
+                N.free(frames_p[i])
+            else:
+                buf = (C.c_uint8 * max(1, lens[i])).from_address(frames_p[i])
+                weakref.finalize(buf, N.free, frames_p[i])
+                frames.append(np.frombuffer(buf, np.uint8, count=lens[i]))
+        N.check(s)
+        return frames
+
     def set_block_mode(self, mode: int):
         N.check(N.batch_set_block_mode(self.handle, int(mode)))
 

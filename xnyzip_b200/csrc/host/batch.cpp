@@ -246,4 +246,30 @@ xnyz_status xnyz_batch_decompress(xnyz_batch* b, uint64_t count, const uint8_t* 
         item_status);
 }
 
+xnyz_status xnyz_batch_roundtrip(xnyz_batch* b, uint64_t count, const float* const* xyz, const uint64_t* n,
+                                 const xnyz_params* params, uint8_t** frame, uint64_t* frame_len, float* const* out,
+                                 xnyz_status* item_status) {
+    if (!b || (count && (!xyz || !n || !params || !frame || !frame_len || !out)))
+        return xnyz::set_last_error(XNYZ_ERR_INVALID_ARG, "null argument");
+    for (uint64_t i = 0; i < count; ++i) {
+        frame[i] = nullptr;
+        frame_len[i] = 0;
+    }
+    const auto order = largest_first(count, [&](uint64_t i) { return n[i]; });
+    return run_pool(
+        b, order,
+        [&](xnyz_ctx* c, uint64_t i) {
+            xnyz_status s = xnyz_compress(c, xyz[i], n[i], 0, &params[i], 1, &frame[i], &frame_len[i], nullptr,
+                                          nullptr);
+            if (s != XNYZ_OK) return s;
+            uint64_t got = 0;
+            s = xnyz_decompress_into(c, frame[i], frame_len[i], 1, params[i].quantizer, params[i].l2_bound,
+                                     params[i].rle, out[i], n[i], &got);
+            if (s == XNYZ_OK && got != n[i])
+                return xnyz::set_last_error(XNYZ_ERR_BAD_STREAM, "round trip changed the point count");
+            return s;
+        },
+        item_status);
+}
+
 }  // extern "C"
