@@ -117,6 +117,17 @@ xnyz_status xnyz_compress(xnyz_ctx* ctx, const float* xyz, uint64_t n, int xyz_i
 xnyz_status xnyz_compress_device(xnyz_ctx* ctx, const float* xyz, uint64_t n, const xnyz_params* params,
                                  const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info);
 
+/* No counterpart in the reference, which decodes its zstd frames with libzstd on the CPU
+ * (composer/utils.hpp:11-33).  Decodes `count` zstd frames on the GPU, one frame per thread:
+ * dev_frames[i] (device memory, frame_len[i] bytes) into dev_out[i] (device memory, out_cap[i]
+ * bytes); out_len[i] receives the content size, or a negative code for a frame that did not
+ * decode (then the call returns XNYZ_ERR_BAD_STREAM).  The pointer and size arrays are host
+ * memory.  Workspace: about 137 KB per frame in the context's workspace.  Frames without a
+ * dictionary only (the container frames have none). */
+xnyz_status xnyz_zstd_decompress_device(xnyz_ctx* ctx, uint64_t count, const uint8_t* const* dev_frames,
+                                        const uint64_t* frame_len, uint8_t* const* dev_out, const uint64_t* out_cap,
+                                        int64_t* out_len);
+
 /* Shared codebooks <- BlockCompressor<float>::fit_profile / compress_with_profile
  * (composer/block_compressor.hpp:241-431) and the profile blob of serialize_profile /
  * deserialize_profile (composer/block_encoding_profile.hpp:17-72): [u32 LE length][repos

@@ -257,6 +257,18 @@ class Context:
                                     int(bool(rle)), C.byref(p), C.byref(n)))
         return p.value, n.value
 
+    def zstd_decompress_device(self, frame_ptrs, frame_lens, out_ptrs, out_caps) -> np.ndarray:
+        """Decodes zstd frames in device memory on the GPU (xnyz_zstd_decompress_device); returns
+        the content sizes as int64."""
+        k = len(frame_ptrs)
+        arrs = [np.ascontiguousarray(a, dtype=np.uint64) for a in (frame_ptrs, frame_lens, out_ptrs, out_caps)]
+        if any(a.shape != (k,) for a in arrs):
+            raise ValueError("one pointer, length, output and capacity per frame")
+        out = np.zeros(k, np.int64)
+        N.check(N.zstd_decompress_device(self.handle, k, *(a.ctypes.data_as(C.c_void_p) for a in arrs),
+                                         out.ctypes.data_as(C.c_void_p)))
+        return out
+
 
 class Batch:
     """Many independent clouds at once (xnyz_batch_*): a pool of worker threads, each with

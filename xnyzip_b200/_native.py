@@ -92,6 +92,7 @@ batch_workers = _proto("xnyz_batch_workers", [_p])
 batch_compress = _proto("xnyz_batch_compress", [_p, C.c_uint64, _p, _p, C.c_int, _p, C.c_int, _p, _p, _p])
 batch_decompress = _proto("xnyz_batch_decompress", [_p, C.c_uint64, _p, _p, C.c_int, _p, _p, _p, _p, _p, _p, _p])
 batch_roundtrip = _proto("xnyz_batch_roundtrip", [_p, C.c_uint64, _p, _p, _p, _p, _p, _p, _p])
+zstd_decompress_device = _proto("xnyz_zstd_decompress_device", [_p, C.c_uint64, _p, _p, _p, _p, _p])
 profile = _proto("xnyz_profile", [_p, C.c_int])
 profile_read = _proto("xnyz_profile_read", [_p, C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)])
 host_hilbert = _proto("xnyz_host_hilbert", [_p, C.c_uint64, C.c_uint, C.c_int, _p])
@@ -141,7 +142,7 @@ EXPORTED = [
     "xnyz_host_free", "xnyz_trim", "xnyz_compress", "xnyz_compress_device", "xnyz_decompress",
     "xnyz_decompress_device", "xnyz_free", "xnyz_stage_quantize", "xnyz_stage_recover", "xnyz_stage_hilbert",
     "xnyz_stage_sort", "xnyz_host_hilbert", "xnyz_host_codebook", "xnyz_profile", "xnyz_profile_read", "xnyz_fit_profile", "xnyz_compress_with_profile", "xnyz_sort_noalloc", "xnyz_decompress_into",
-    "xnyz_batch_create", "xnyz_batch_destroy", "xnyz_batch_workers", "xnyz_batch_compress", "xnyz_batch_decompress", "xnyz_batch_roundtrip",
+    "xnyz_batch_create", "xnyz_batch_destroy", "xnyz_batch_workers", "xnyz_batch_compress", "xnyz_batch_decompress", "xnyz_batch_roundtrip", "xnyz_zstd_decompress_device",
     "xnyz_set_block_mode", "xnyz_set_model", "xnyz_model_param_count", "xnyz_last_block_info",
     "xnyz_batch_set_block_mode", "xnyz_stage_repos", "xnyz_block_features", "xnyz_block_search", "xnyz_block_cost",
     "xnyz_mlp_forward", "xnyz_mlp_gather_floats", "xnyz_mlp_train_batch", "xnyz_mlp_adam",

@@ -1976,6 +1976,43 @@ xnyz_status xnyz_decompress_into(xnyz_ctx* c, const uint8_t* in, uint64_t in_len
     return XNYZ_OK;
 }
 
+xnyz_status xnyz_zstd_decompress_device(xnyz_ctx* c, uint64_t count, const uint8_t* const* dev_frames,
+                                        const uint64_t* frame_len, uint8_t* const* dev_out, const uint64_t* out_cap,
+                                        int64_t* out_len) {
+    clear_stale_cuda_error();
+    if (!c || (count && (!dev_frames || !frame_len || !dev_out || !out_cap || !out_len)))
+        return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!count) return XNYZ_OK;
+    cudaStream_t st = c->stream;
+    Plan pl;
+    const size_t o_arr = pl.add(40 * count);  // src | src_len | dst | cap | out_len
+    const size_t o_ws = pl.add(zstd_workspace_bytes() * count);
+    TRY(ensure_arena(c, pl.total));
+    TRY(ensure_host_stage(c, 40 * count));
+    uint64_t* h = reinterpret_cast<uint64_t*>(c->h_stage);
+    std::memcpy(h, dev_frames, 8 * count);
+    std::memcpy(h + count, frame_len, 8 * count);
+    std::memcpy(h + 2 * count, dev_out, 8 * count);
+    std::memcpy(h + 3 * count, out_cap, 8 * count);
+    uint64_t* d = at<uint64_t>(c, o_arr);
+    CUDA_TRY(cudaMemcpyAsync(d, h, 32 * count, cudaMemcpyHostToDevice, st));
+    launch_zstd_frames(reinterpret_cast<const uint8_t* const*>(d), d + count, reinterpret_cast<uint8_t* const*>(d + 2 * count),
+                       d + 3 * count, reinterpret_cast<long long*>(d + 4 * count), at<char>(c, o_ws), count, st);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(h + 4 * count, d + 4 * count, 8 * count, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    uint64_t bad = count;
+    for (uint64_t i = 0; i < count; ++i) {
+        out_len[i] = static_cast<int64_t>(h[4 * count + i]);
+        if (out_len[i] < 0 && bad == count) bad = i;
+    }
+    if (bad != count)
+        return fail(XNYZ_ERR_BAD_STREAM, "zstd frame " + std::to_string(bad) + " did not decode (" +
+                                             std::to_string(out_len[bad]) + ")");
+    return XNYZ_OK;
+}
+
 xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, uint64_t len, int quantizer,
                                    float l2_bound, int rle, const float** dev_xyz, uint64_t* n) {
     clear_stale_cuda_error();

@@ -285,5 +285,12 @@ void launch_mlp_train(const float* prm, const float* feats, const uint8_t* wlab,
                       float* gather, cudaStream_t st);
 void launch_mlp_adam(float* prm, float* grad, float* m, float* v, float lr, int step, cudaStream_t st);
 
+// zstd frames on the GPU (k_zstd.cu): frame i of src_len[i] bytes at src[i] into dst[i]
+// (capacity cap[i]); out_len[i] = content size or < 0 (zstd_dec.cuh error codes).  The
+// pointer and size arrays are in device memory; `workspace` holds count * zstd_workspace_bytes().
+size_t zstd_workspace_bytes();
+void launch_zstd_frames(const uint8_t* const* src, const uint64_t* src_len, uint8_t* const* dst, const uint64_t* cap,
+                        long long* out_len, void* workspace, uint64_t count, cudaStream_t st);
+
 }  // namespace dev
 }  // namespace xnyz
