@@ -118,7 +118,7 @@ xnyz_status xnyz_compress_device(xnyz_ctx* ctx, const float* xyz, uint64_t n, co
                                  const uint8_t** dev_container, uint64_t* container_len, xnyz_compress_info* info);
 
 /* No counterpart in the reference, which decodes its zstd frames with libzstd on the CPU
- * (composer/utils.hpp:11-33).  Decodes `count` zstd frames on the GPU, one frame per thread:
+ * (composer/utils.hpp:11-33).  Decodes `count` zstd frames on the GPU, one frame per warp:
  * dev_frames[i] (device memory, frame_len[i] bytes) into dev_out[i] (device memory, out_cap[i]
  * bytes); out_len[i] receives the content size, or a negative code for a frame that did not
  * decode (then the call returns XNYZ_ERR_BAD_STREAM).  The pointer and size arrays are host

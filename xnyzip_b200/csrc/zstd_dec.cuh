@@ -5,7 +5,14 @@
 // Supported: single zstd frames without dictionary, raw / RLE / compressed blocks, raw / RLE /
 // Huffman (1 or 4 streams, tree or repeated tree) literals, predefined / RLE / FSE / repeated
 // sequence tables, repeat offsets, an optional content checksum (skipped, not verified).
-// One call decodes one frame sequentially; the GPU kernel runs one frame per thread.
+//
+// A Team is the set of threads that decode one frame together.  On the GPU it is a warp:
+// every lane runs every step on the same data (the same branches; same-address loads are
+// broadcasts), and only the stores are split: byte copies and Huffman table fills go
+// lane-strided, the four Huffman literal streams go to lanes 0-3, FSE tables are built by
+// lane 0, and a warp barrier separates each batch of stores from the reads that follow.
+// Every branch depends only on values that all lanes hold alike, so the lanes never diverge
+// around a barrier.  On the host a Team is one thread (SoloTeam).
 #pragma once
 
 #include <cstdint>
@@ -45,9 +52,40 @@ struct Workspace {
     u8 lit[kMaxBlock + 32];
     u16 huf[1 << kHufMaxBits];  // (symbol << 8) | bits
     FseEntry ll[512], of[256], ml[512];
-    int huf_bits;               // 0: no table yet
-    int ll_log, of_log, ml_log; // -1: no table yet
 };
+// Table sizes of the frame so far, held by each thread of the team.
+struct Logs {
+    int huf_bits = 0;                      // 0: no Huffman table yet
+    int ll = -1, of = -1, ml = -1;         // -1: no sequence table yet
+};
+
+// One host thread.
+struct SoloTeam {
+    int rank = 0;
+    static constexpr int size = 1;
+    void sync() const {}
+    int min(int v) const { return v; }
+    int bcast0(int v) const { return v; }
+};
+
+#ifdef __CUDACC__
+// One warp (all 32 lanes active).  sync() puts a block-scope fence between two warp
+// barriers: with the barrier alone, lanes still copying one block's last literals read
+// bytes that another lane had already overwritten with the next block's literals (seen on
+// sm_100a in one of the test frames); with the fence every lane's earlier loads and stores
+// are performed before any lane goes on.
+struct WarpTeam {
+    int rank;
+    static constexpr int size = 32;
+    __device__ __forceinline__ void sync() const {
+        __syncwarp();
+        __threadfence_block();
+        __syncwarp();
+    }
+    __device__ __forceinline__ int min(int v) const { return __reduce_min_sync(0xffffffffu, v); }
+    __device__ __forceinline__ int bcast0(int v) const { return __shfl_sync(0xffffffffu, v, 0); }
+};
+#endif
 
 // ---- little-endian reads ----
 ZD_HD u32 rd16(const u8* p) { return (u32)p[0] | ((u32)p[1] << 8); }
@@ -69,9 +107,12 @@ struct BackBits {
     i64 len;    // bytes
     i64 pos;    // bits not yet consumed (from bit 0 of buf)
     i64 total;  // bits after the padding
+    i64 wb;     // first byte of the cached 8-byte window
+    u64 win;    // buf[wb .. wb+8), bytes outside the buffer as zero
     ZD_HD bool init(const u8* b, u64 n) {
         buf = b;
         len = (i64)n;
+        wb = -(1ll << 40);
         if (!n || !b[n - 1]) return false;
         total = (i64)n * 8 - 8 + highbit(b[n - 1]);
         pos = total;
@@ -83,17 +124,23 @@ struct BackBits {
         pos -= n;
         return peek_at(pos, n);
     }
-    ZD_HD u32 peek(int n) const { return n ? peek_at(pos - n, n) : 0; }
-    ZD_HD u32 peek_at(i64 p, int n) const {
-        u64 v = 0;
+    ZD_HD u32 peek(int n) { return n ? peek_at(pos - n, n) : 0; }
+    // The bits [p, p+n) need bytes p/8 .. p/8+4; the window is refilled 3 bytes below p/8,
+    // so the reads that follow (towards the start) hit it for about 32 bits.
+    ZD_HD u32 peek_at(i64 p, int n) {
         const i64 byte0 = p >> 3;  // arithmetic shift: negative positions round down
-        for (int k = 0; k < 6; ++k) {
-            const i64 b = byte0 + k;
-            const u64 x = (b >= 0 && b < len) ? buf[b] : 0;
-            v |= x << (8 * k);
+        if (byte0 < wb || byte0 > wb + 3) {
+            wb = byte0 - 3;
+            u64 v = 0;
+            for (int k = 0; k < 8; ++k) {
+                const i64 b = wb + k;
+                const u64 x = (b >= 0 && b < len) ? buf[b] : 0;
+                v |= x << (8 * k);
+            }
+            win = v;
         }
-        const int sh = (int)(p - byte0 * 8);
-        return (u32)((v >> sh) & ((1ull << n) - 1));
+        const int sh = (int)(p - wb * 8);
+        return (u32)((win >> sh) & ((1ull << n) - 1));
     }
     ZD_HD bool overflow() const { return pos < 0; }
 };
@@ -240,7 +287,8 @@ ZD_HD void ml_code(int c, u32& base, int& bits) {
 
 // ---- Huffman literals ----
 // Tree description (RFC 8878 4.2.1) -> ws.huf; returns bytes used or < 0.
-ZD_HD int read_huf_tree(const u8* src, u64 len, Workspace& ws) {
+template <class Team>
+ZD_HD int read_huf_tree(const u8* src, u64 len, Workspace& ws, int& huf_bits, const Team& team) {
     if (len < 1) return kErrTruncated;
     u8 w[256];
     int nw = 0;
@@ -307,20 +355,21 @@ ZD_HD int read_huf_tree(const u8* src, u64 len, Workspace& ws) {
         if (!k) continue;
         const u32 span = 1u << (k - 1);
         const u16 e = (u16)((s << 8) | (maxb + 1 - k));
-        for (u32 j = 0; j < span; ++j) ws.huf[start[k] + j] = e;
+        for (u32 j = team.rank; j < span; j += team.size) ws.huf[start[k] + j] = e;
         start[k] += span;
     }
-    ws.huf_bits = maxb;
+    huf_bits = maxb;
+    team.sync();
     return (int)used;
 }
 
-ZD_HD int huf_stream(const u8* src, u64 len, u8* out, u64 n, const Workspace& ws) {
+// Decodes n literals; stores out[i] only where (i & wmask) == wrank.
+ZD_HD int huf_stream(const u8* src, u64 len, u8* out, u64 n, const Workspace& ws, int mb, u64 wmask, u64 wrank) {
     BackBits bb;
     if (!bb.init(src, len)) return kErrFormat;
-    const int mb = ws.huf_bits;
     for (u64 i = 0; i < n; ++i) {
         const u16 e = ws.huf[bb.peek(mb)];
-        out[i] = (u8)(e >> 8);
+        if ((i & wmask) == wrank) out[i] = (u8)(e >> 8);
         bb.pos -= (e & 0xff);
     }
     if (bb.pos != 0) return kErrFormat;
@@ -328,7 +377,10 @@ ZD_HD int huf_stream(const u8* src, u64 len, u8* out, u64 n, const Workspace& ws
 }
 
 // Literals section; returns bytes used or < 0, *nlit = regenerated size.
-ZD_HD int read_literals(const u8* src, u64 len, Workspace& ws, u64& nlit) {
+// The literals are in ws.lit for every lane when it returns.
+template <class Team>
+ZD_HD int read_literals(const u8* src, u64 len, Workspace& ws, int& huf_bits, u64& nlit, const Team& team) {
+    team.sync();  // every lane is done with the previous block's literals
     if (len < 1) return kErrTruncated;
     const int type = src[0] & 3, fmt = (src[0] >> 2) & 3;
     if (type < 2) {
@@ -348,12 +400,14 @@ ZD_HD int read_literals(const u8* src, u64 len, Workspace& ws, u64& nlit) {
         if (n > kMaxBlock) return kErrFormat;
         if (type == 0) {
             if (h + n > len) return kErrTruncated;
-            for (u64 i = 0; i < n; ++i) ws.lit[i] = src[h + i];
+            for (u64 i = team.rank; i < n; i += team.size) ws.lit[i] = src[h + i];
+            team.sync();
             nlit = n;
             return (int)(h + n);
         }
         if (h + 1 > len) return kErrTruncated;
-        for (u64 i = 0; i < n; ++i) ws.lit[i] = src[h];
+        for (u64 i = team.rank; i < n; i += team.size) ws.lit[i] = src[h];
+        team.sync();
         nlit = n;
         return (int)(h + 1);
     }
@@ -382,15 +436,16 @@ ZD_HD int read_literals(const u8* src, u64 len, Workspace& ws, u64& nlit) {
     const u8* p = src + h;
     u64 rem = comp;
     if (type == 2) {
-        const int r = read_huf_tree(p, rem, ws);
+        const int r = read_huf_tree(p, rem, ws, huf_bits, team);
         if (r < 0) return r;
         p += r;
         rem -= (u64)r;
-    } else if (!ws.huf_bits) {
+    } else if (!huf_bits) {
         return kErrFormat;  // repeated tree without a previous one
     }
     if (streams == 1) {
-        const int r = huf_stream(p, rem, ws.lit, regen, ws);
+        const int r = huf_stream(p, rem, ws.lit, regen, ws, huf_bits, (u64)team.size - 1, (u64)team.rank);
+        team.sync();
         if (r < 0) return r;
     } else {
         if (rem < 6) return kErrTruncated;
@@ -399,24 +454,33 @@ ZD_HD int read_literals(const u8* src, u64 len, Workspace& ws, u64& nlit) {
         const u64 s4 = rem - 6 - s1 - s2 - s3;
         const u64 seg = (regen + 3) / 4;
         if (3 * seg > regen) return kErrFormat;
-        const u8* q = p + 6;
         const u64 sz[4] = {s1, s2, s3, s4};
-        u64 off = 0;
-        for (int k = 0; k < 4; ++k) {
+        // a one-thread team decodes the four streams in turn; a warp gives stream k to the
+        // lanes k, k+4, ... of which lane k stores
+        const int first = team.size == 1 ? 0 : (team.rank & 3);
+        const int step = team.size == 1 ? 1 : 4;
+        const u64 wrank = team.rank < 4 ? 0 : 1;
+        int worst = kOk;
+        for (int k = first; k < 4; k += step) {
+            u64 start = 6;
+            for (int j = 0; j < k; ++j) start += sz[j];
             const u64 cnt = k < 3 ? seg : regen - 3 * seg;
-            const int r = huf_stream(q, sz[k], ws.lit + off, cnt, ws);
-            if (r < 0) return r;
-            q += sz[k];
-            off += cnt;
+            const int r = huf_stream(p + start, sz[k], ws.lit + (u64)k * seg, cnt, ws, huf_bits, 0, wrank);
+            if (r < worst) worst = r;
         }
+        worst = team.min(worst);
+        team.sync();
+        if (worst < 0) return worst;
     }
     nlit = regen;
     return (int)(h + comp);
 }
 
 // Sequence table for one of LL / OF / ML by its mode; returns bytes used or < 0.
+// The table is built by rank 0; every lane sees it when this returns.
+template <class Team>
 ZD_HD int read_table(int mode, const u8* src, u64 len, FseEntry* t, int& log, int max_log, int max_sym,
-                     int which) {
+                     int which, const Team& team) {
     if (mode == 0) {
         short norm[64];
         if (which == 0) default_ll(norm);
@@ -424,12 +488,17 @@ ZD_HD int read_table(int mode, const u8* src, u64 len, FseEntry* t, int& log, in
         else default_ml(norm);
         const int nsym = which == 0 ? 36 : which == 1 ? 29 : 53;
         log = which == 1 ? 5 : 6;
-        return build_fse(norm, nsym, log, t) == kOk ? 0 : kErrFormat;
+        int rc = kOk;
+        if (team.rank == 0) rc = build_fse(norm, nsym, log, t);
+        rc = team.bcast0(rc);
+        team.sync();
+        return rc == kOk ? 0 : kErrFormat;
     }
     if (mode == 1) {
         if (len < 1) return kErrTruncated;
         if (src[0] > max_sym) return kErrFormat;
-        rle_fse(t, src[0]);
+        if (team.rank == 0) rle_fse(t, src[0]);
+        team.sync();
         log = 0;
         return 1;
     }
@@ -438,16 +507,22 @@ ZD_HD int read_table(int mode, const u8* src, u64 len, FseEntry* t, int& log, in
         int nsym = 0;
         const int r = read_ncount(src, len, max_log, max_sym, norm, nsym, log);
         if (r < 0) return r;
-        if (build_fse(norm, nsym, log, t) != kOk) return kErrFormat;
+        int rc = kOk;
+        if (team.rank == 0) rc = build_fse(norm, nsym, log, t);
+        rc = team.bcast0(rc);
+        team.sync();
+        if (rc != kOk) return kErrFormat;
         return r;
     }
     return log < 0 ? kErrFormat : 0;  // repeat the previous table
 }
 
 // One compressed block into dst[op ...]; returns bytes written or < 0.
-ZD_HD i64 decode_block(const u8* src, u64 len, u8* dst, u64 op, u64 cap, Workspace& ws, u32* rep) {
+template <class Team>
+ZD_HD i64 decode_block(const u8* src, u64 len, u8* dst, u64 op, u64 cap, Workspace& ws, Logs& lg, u32* rep,
+                       const Team& team) {
     u64 nlit = 0;
-    const int lr = read_literals(src, len, ws, nlit);
+    const int lr = read_literals(src, len, ws, lg.huf_bits, nlit, team);
     if (lr < 0) return lr;
     const u8* p = src + lr;
     u64 rem = len - (u64)lr;
@@ -475,29 +550,30 @@ ZD_HD i64 decode_block(const u8* src, u64 len, u8* dst, u64 op, u64 cap, Workspa
     u64 o = op;
     if (nseq == 0) {
         if (o + nlit > cap) return kErrDstSize;
-        for (u64 i = 0; i < nlit; ++i) dst[o + i] = ws.lit[i];
+        for (u64 i = team.rank; i < nlit; i += team.size) dst[o + i] = ws.lit[i];
         return (i64)nlit;
     }
     if (rem < 1) return kErrTruncated;
     const int modes = p[0];
     p += 1;
     rem -= 1;
-    int r = read_table(modes >> 6, p, rem, ws.ll, ws.ll_log, 9, 35, 0);
+    int r = read_table(modes >> 6, p, rem, ws.ll, lg.ll, 9, 35, 0, team);
     if (r < 0) return r;
     p += r;
     rem -= (u64)r;
-    r = read_table((modes >> 4) & 3, p, rem, ws.of, ws.of_log, 8, 31, 1);
+    r = read_table((modes >> 4) & 3, p, rem, ws.of, lg.of, 8, 31, 1, team);
     if (r < 0) return r;
     p += r;
     rem -= (u64)r;
-    r = read_table((modes >> 2) & 3, p, rem, ws.ml, ws.ml_log, 9, 52, 2);
+    r = read_table((modes >> 2) & 3, p, rem, ws.ml, lg.ml, 9, 52, 2, team);
     if (r < 0) return r;
     p += r;
     rem -= (u64)r;
     BackBits bb;
     if (!bb.init(p, rem)) return kErrFormat;
-    u32 sll = bb.read(ws.ll_log), sof = bb.read(ws.of_log), sml = bb.read(ws.ml_log);
+    u32 sll = bb.read(lg.ll), sof = bb.read(lg.of), sml = bb.read(lg.ml);
     u64 li = 0;
+    u64 synced = o;  // every lane sees the output below this position
     for (u64 k = 0; k < nseq; ++k) {
         const int llc = ws.ll[sll].sym, ofc = ws.of[sof].sym, mlc = ws.ml[sml].sym;
         if (ofc > 31) return kErrFormat;
@@ -541,22 +617,35 @@ ZD_HD i64 decode_block(const u8* src, u64 len, u8* dst, u64 op, u64 cap, Workspa
             sof = ws.of[sof].base + bb.read(ws.of[sof].nb);
         }
         if (li + ll > nlit || o + ll + ml > cap) return li + ll > nlit ? kErrFormat : kErrDstSize;
-        for (u32 i = 0; i < ll; ++i) dst[o + i] = ws.lit[li + i];
+        for (u32 i = team.rank; i < ll; i += team.size) dst[o + i] = ws.lit[li + i];
         o += ll;
         li += ll;
         if (off > o) return kErrFormat;
+        // Byte i of the match repeats byte i mod off of the off bytes before it, all written
+        // before this match: the lanes copy in any order once those bytes are visible, which
+        // needs a barrier only when the sources reach past the last one.
         const u64 from = o - off;
-        for (u32 i = 0; i < ml; ++i) dst[o + i] = dst[from + i];
+        if (from + (off < ml ? off : ml) > synced) {
+            team.sync();
+            synced = o;
+        }
+        if (off >= ml) {
+            for (u32 i = team.rank; i < ml; i += team.size) dst[o + i] = dst[from + i];
+        } else {
+            for (u32 i = team.rank; i < ml; i += team.size) dst[o + i] = dst[from + i % off];
+        }
         o += ml;
     }
     if (bb.pos != 0) return kErrFormat;
     if (o + (nlit - li) > cap) return kErrDstSize;
-    for (u64 i = li; i < nlit; ++i) dst[o++] = ws.lit[i];
+    for (u64 i = li + team.rank; i < nlit; i += team.size) dst[o + (i - li)] = ws.lit[i];
+    o += nlit - li;
     return (i64)(o - op);
 }
 
 // One frame: src[0..len) -> dst[0..cap); returns the content size or < 0.
-ZD_HD i64 decode_frame(const u8* src, u64 len, u8* dst, u64 cap, Workspace& ws) {
+template <class Team>
+ZD_HD i64 decode_frame(const u8* src, u64 len, u8* dst, u64 cap, Workspace& ws, const Team& team) {
     if (len < 6 || rd32(src) != 0xFD2FB528u) return kErrFormat;
     const u32 fhd = src[4];
     const int fcs_flag = fhd >> 6, single = (fhd >> 5) & 1, checksum = (fhd >> 2) & 1, did = fhd & 3;
@@ -573,8 +662,7 @@ ZD_HD i64 decode_frame(const u8* src, u64 len, u8* dst, u64 cap, Workspace& ws) 
     else if (fcs_bytes == 4) fcs = rd32(src + p);
     else if (fcs_bytes == 8) fcs = (u64)rd32(src + p) | ((u64)rd32(src + p + 4) << 32);
     p += fcs_bytes;
-    ws.huf_bits = 0;
-    ws.ll_log = ws.of_log = ws.ml_log = -1;
+    Logs lg;
     u32 rep[3] = {1, 4, 8};
     u64 o = 0;
     for (;;) {
@@ -587,18 +675,18 @@ ZD_HD i64 decode_frame(const u8* src, u64 len, u8* dst, u64 cap, Workspace& ws) 
         if (type == 0) {
             if (p + bsize > len) return kErrTruncated;
             if (o + bsize > cap) return kErrDstSize;
-            for (u64 i = 0; i < bsize; ++i) dst[o + i] = src[p + i];
+            for (u64 i = team.rank; i < bsize; i += team.size) dst[o + i] = src[p + i];
             o += bsize;
             p += bsize;
         } else if (type == 1) {
             if (p + 1 > len) return kErrTruncated;
             if (o + bsize > cap) return kErrDstSize;
-            for (u64 i = 0; i < bsize; ++i) dst[o + i] = src[p];
+            for (u64 i = team.rank; i < bsize; i += team.size) dst[o + i] = src[p];
             o += bsize;
             p += 1;
         } else {
             if (bsize > kMaxBlock || p + bsize > len) return kErrTruncated;
-            const i64 w = decode_block(src + p, bsize, dst, o, cap, ws, rep);
+            const i64 w = decode_block(src + p, bsize, dst, o, cap, ws, lg, rep, team);
             if (w < 0) return w;
             o += (u64)w;
             p += bsize;
