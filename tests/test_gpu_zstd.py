@@ -110,3 +110,31 @@ def test_damaged_frames(ctx, xnyz):
             _gpu_decode(ctx, frames, caps)
     lens, outs, _, _ = _gpu_decode(ctx, [f], [len(data)])
     assert lens[0] == len(data) and outs[0] == data
+
+
+def test_random_frames(ctx):
+    """48 seeded frames of mixed random, run, geometric and repeated data (up to ~1.5 MB, levels
+    1-19), decoded in one call: every frame equals libzstd's input."""
+    z = _libzstd()
+    rng = np.random.default_rng(2024)
+    data, frames = [], []
+    for _ in range(48):
+        parts, total, want = [], 0, int(rng.integers(1000, 1_500_000))
+        while total < want:
+            kind, n = int(rng.integers(0, 4)), int(rng.integers(1, 50000))
+            if kind == 0:
+                p = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
+            elif kind == 1:
+                p = bytes([int(rng.integers(0, 256))]) * n
+            elif kind == 2:
+                p = rng.geometric(float(rng.uniform(0.05, 0.9)), n).astype(np.uint8).tobytes()
+            else:
+                p = parts[int(rng.integers(0, len(parts)))][:n] if parts else b"abc"
+            parts.append(p)
+            total += len(p)
+        d = b"".join(parts)
+        data.append(d)
+        frames.append(_zstd(z, d, int(rng.choice([1, 2, 3, 5, 9, 15, 19]))))
+    lens, outs, _, _ = _gpu_decode(ctx, frames, [len(d) for d in data])
+    assert list(lens) == [len(d) for d in data]
+    assert [i for i, (o, d) in enumerate(zip(outs, data)) if o != d] == []
