@@ -363,6 +363,14 @@ def run_gpu(args):
     if args.batch_clouds and rank == 0 and world == 1:
         batched = batched_measure(ctx, stream, dev, args.batch_clouds, args.workers)
 
+    # ---- zstd frames decoded on the GPU ----
+    zstd_frames = None
+    if args.zstd_frames and rank == 0 and world == 1:
+        try:
+            zstd_frames = zstd_measure(ctx, stream, dev, count=args.zstd_frames)
+        except Exception as e:  # reported in the line, the rest of it stands
+            zstd_frames = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- CPU baseline: the reference on a bounded sample (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -441,6 +449,8 @@ def run_gpu(args):
             line["learned"] = learned
         if batched is not None:
             line["batched"] = batched
+        if zstd_frames is not None:
+            line["zstd_frames"] = zstd_frames
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -581,6 +591,84 @@ def batched_measure(ctx, stream, dev, count, workers):
     return out
 
 
+# ------------------------------------------------------------- zstd frames on the GPU ---
+def zstd_measure(ctx, stream, dev, points=4_000_000, piece=1 << 16, count=6360, reps=3):
+    """xnyz_zstd_decompress_device on many small frames: the pre-zstd container of a
+    `points`-point terrain cloud (TO, L2 0.01, Hilbert, -rle) cut into `piece`-byte pieces, each
+    a libzstd 1.5.7 level-3 frame, repeated to `count` frames.  Device time with CUDA events on
+    the context's stream (best of `reps`), the output compared bit for bit on the device; host
+    libzstd (ZSTD_decompress) on the same frames with one thread and with every host thread."""
+    import concurrent.futures as cf
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from xnyzip_b200 import _native as N
+    z = C.CDLL(N.default_zstd_library())
+    z.ZSTD_compressBound.restype = C.c_size_t
+    z.ZSTD_compressBound.argtypes = [C.c_size_t]
+    z.ZSTD_compress.restype = C.c_size_t
+    z.ZSTD_compress.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int]
+    z.ZSTD_decompress.restype = C.c_size_t
+    z.ZSTD_decompress.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]
+
+    def frame(b):
+        cap = z.ZSTD_compressBound(len(b))
+        out = C.create_string_buffer(cap)
+        size = z.ZSTD_compress(out, cap, b, len(b), 3)  # before reading out.raw, which copies
+        return out.raw[:size]
+
+    plain = ctx.compress(make_cloud("terrain", points, 7), 1, 0.01, True, True, use_zstd=False)
+    pieces = [plain[i:i + piece] for i in range(0, len(plain), piece)]
+    uniq = [frame(b) for b in pieces]
+    k = -(-count // len(pieces))
+    frames, content = (uniq * k)[:count], (pieces * k)[:count]
+    caps = [len(b) for b in content]
+    total = float(sum(caps))
+    src = torch.frombuffer(bytearray(b"".join(frames)), dtype=torch.uint8).to(dev)
+    ref = torch.frombuffer(bytearray(b"".join(content)), dtype=torch.uint8).to(dev)
+    dst = torch.empty_like(ref)
+    torch.cuda.synchronize(dev)  # the copies above ran on torch's stream, the decoder runs on the context's
+    f_off = np.cumsum([0] + [len(f) for f in frames])[:-1]
+    d_off = np.cumsum([0] + caps)[:-1]
+    call = ([src.data_ptr() + int(o) for o in f_off], [len(f) for f in frames],
+            [dst.data_ptr() + int(o) for o in d_off], caps)
+    ctx.zstd_decompress_device(*call)  # sizes the workspace
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lens = ctx.zstd_decompress_device(*call)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    exact = list(lens) == caps and bool(torch.equal(dst, ref))
+
+    def host(idx):
+        buf = C.create_string_buffer(piece)
+        for i in idx:
+            if z.ZSTD_decompress(buf, piece, frames[i], len(frames[i])) != caps[i]:
+                raise RuntimeError("libzstd size mismatch")
+
+    t = time.perf_counter()
+    host(range(len(frames)))
+    cpu1 = total / (time.perf_counter() - t)
+    threads = os.cpu_count() or 1
+    with cf.ThreadPoolExecutor(threads) as ex:
+        t = time.perf_counter()
+        list(ex.map(host, [range(j, len(frames), threads) for j in range(threads)]))
+        cpun = total / (time.perf_counter() - t)
+    del src, ref, dst
+    torch.cuda.empty_cache()
+    return {"frames": len(frames), "frame_content_bytes": piece, "content_bytes": int(total),
+            "compressed_bytes": int(sum(len(f) for f in frames)), "gpu_GB_s": round(total / min(ts) / 1e9, 3),
+            "gpu_ms": round(min(ts) * 1e3, 3), "rep_ms": [round(x * 1e3, 3) for x in ts], "bit_exact": exact,
+            "host_libzstd_GB_s": {"1": round(cpu1 / 1e9, 3), str(threads): round(cpun / 1e9, 3)},
+            "workload": f"pre-zstd container of a {points}-point terrain cloud (TO 0.01, Hilbert, -rle) in "
+                        f"{piece}-byte pieces, each a libzstd level-3 frame, repeated to {count} frames; "
+                        "one warp per frame"}
+
+
 # ---------------------------------------------------------------------- CPU baselines ---
 def _ref_lib():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -689,6 +777,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-clouds", type=int, default=2048,
                     help="clouds of the uneven batch workload (0: skip that measurement)")
+    ap.add_argument("--zstd-frames", type=int, default=6360,
+                    help="frames of the GPU zstd decoding measurement (0: skip it)")
+    ap.add_argument("--zstd-only", action="store_true",
+                    help="run only the GPU zstd decoding measurement and print it")
     ap.add_argument("--learned", action=argparse.BooleanOptionalAction, default=True,
                     help="also measure the extended container with learned block parameters")
     args = ap.parse_args()
@@ -696,6 +788,14 @@ def main():
         log("warning: fewer than 3 warm-up steps")
     if args.impl == "reference":
         run_reference(args)
+    elif args.zstd_only:
+        import torch
+        import xnyzip_b200 as X
+        stream = torch.cuda.Stream()
+        ctx = X.Context(0, stream=stream.cuda_stream)
+        print(json.dumps({"zstd_frames": zstd_measure(ctx, stream, torch.device("cuda", 0),
+                                                      count=args.zstd_frames or 6360)}), flush=True)
+        ctx.close()
     else:
         run_gpu(args)
 
