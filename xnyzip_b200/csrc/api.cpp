@@ -1982,6 +1982,8 @@ xnyz_status xnyz_zstd_decompress_device(xnyz_ctx* c, uint64_t count, const uint8
     clear_stale_cuda_error();
     if (!c || (count && (!dev_frames || !frame_len || !dev_out || !out_cap || !out_len)))
         return fail(XNYZ_ERR_INVALID_ARG, "null argument");
+    if (count > (uint64_t)1 << 32)  // the workspace alone would be 600 TB; keeps the sizes below from wrapping
+        return fail(XNYZ_ERR_INVALID_ARG, "too many frames in one call");
     CUDA_TRY(cudaSetDevice(c->device));
     if (!count) return XNYZ_OK;
     cudaStream_t st = c->stream;
