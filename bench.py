@@ -134,15 +134,30 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def _synthetic():
+    """The seeded generators, loaded from their file: importing the package would load the
+    CUDA library, which the reference arm must not map."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("xnyz_synthetic", os.path.join(ROOT, "xnyzip_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cloud_seed(workload: str, rank: int) -> int:
+    """Seed of rank `rank`'s cloud (the terrain cloud of rank 0 is seed 1, the spheres seed 2)."""
+    return 1 + rank + (1 if WORKLOADS[workload][0] == "spheres" else 0)
+
+
 def make_cloud(workload: str, n: int, seed: int):
-    from xnyzip_b200 import synthetic as S
+    S = _synthetic()
     if WORKLOADS[workload][0] == "spheres":
-        return S.spheres(n, 200_000, seed + 1)
+        return S.spheres(n, 200_000, seed)
     return S.terrain(n, seed)
 
 
-def workload_config(workload: str, n: int, variants) -> dict:
-    """The workload part of the bench line's config, the same for both arms."""
+def workload_config(workload: str, n: int, variants, world: int = 1) -> dict:
+    """The bench line's config, the same for both arms."""
     return {
         "workload": (f"terrain {n} points, Hilbert, -rle, quantizers to/cube x L2 {{0.001,0.01,0.1}}"
                      if workload == "terrain" else
@@ -151,7 +166,18 @@ def workload_config(workload: str, n: int, variants) -> dict:
         "points": n,
         "variants": [vname(v) for v in variants],
         "direct_threshold": 1024,
+        "l2_flush": f"inputs ({12 * n / 1e6:.0f} MB per cloud) exceed the 126 MB L2",
+        "parallelism": f"replicas x{world}",
     }
+
+
+def load_digests() -> dict:
+    """Reference digests of the full-size clouds (tests/golden/make_ref_digests.py)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "ref_digests.json")) as f:
+            return json.load(f)
+    except FileNotFoundError:
+        return {}
 
 
 class RankSync:
@@ -200,7 +226,8 @@ def run_gpu(args):
 
     n = args.points or WORKLOADS[args.workload][1]
     t0 = time.time()
-    host = make_cloud(args.workload, n, 1 + rank)
+    seed = cloud_seed(args.workload, rank)
+    host = make_cloud(args.workload, n, seed)
     log(f"[rank {rank}] generated {n} points in {time.time() - t0:.1f}s")
     pinned = torch.from_numpy(host).pin_memory()
     d_pts = pinned.to(dev, non_blocking=False)
@@ -324,18 +351,19 @@ def run_gpu(args):
         for vi, v in enumerate(variants):
             chunk_bytes[v] = sum(len(f) for f in frames[vi * len(bounds):(vi + 1) * len(bounds)])
 
+    mono_frames = {}
+
     def e2e_monolithic_step():
         if args.e2e_mode == "roundtrip":
             frames = batch.roundtrip(m_clouds, m_params, outs)
-            for v, f in zip(variants, frames):
-                frame_bytes[v] = len(f)
-            return
-        frames = batch.compress(m_clouds, m_params, as_bytes=False)
-        ns = batch.decompress(frames, m_dparams, outs)
-        if ns != [n] * len(variants):
-            raise RuntimeError("e2e decode size mismatch")
+        else:
+            frames = batch.compress(m_clouds, m_params, as_bytes=False)
+            ns = batch.decompress(frames, m_dparams, outs)
+            if ns != [n] * len(variants):
+                raise RuntimeError("e2e decode size mismatch")
         for v, f in zip(variants, frames):
             frame_bytes[v] = len(f)
+            mono_frames[v] = f  # the last step's frames are checked against the reference below
 
     def timed(fn, steps):
         fn()  # warm-up: worker arenas and pinned staging reach their sizes
@@ -352,6 +380,13 @@ def run_gpu(args):
         e2e_s = timed(e2e_chunked_step, e2e_steps)
         mono_s = timed(e2e_monolithic_step, e2e_steps)
     batch.close()
+
+    # ---- parity of the timed paths with the reference, and the L2 bound of every point ----
+    parity = None
+    if args.parity and rank == 0:
+        parity = parity_measure(ctx, dev, d_pts, host, n, variants, args.workload, seed,
+                                mono_frames if e2e_steps else None, outs if e2e_steps else None)
+    del outs, mono_frames
 
     # ---- learned block parameters (extended container) on the same cloud ----
     learned = None
@@ -405,15 +440,13 @@ def run_gpu(args):
             "dtype": "f32 in, int32/u64 lattice and key arithmetic",
             "data": (f"synthetic {'terrain-LiDAR' if args.workload == 'terrain' else 'clustered-surface'} "
                      f"stand-in (seeded, {n} points), generated on the host"),
-            "config": {
-                **workload_config(args.workload, n, variants),
-                "l2_flush": f"inputs ({12 * n / 1e6:.0f} MB per cloud) exceed the 126 MB L2",
-                "value_path": f"device-resident points and pre-zstd container; the independent variants spread "
-                              f"over {pipes} contexts / streams, CUDA events on the main stream bracketing all",
-                "e2e_path": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
-                            + ("xnyz_batch_roundtrip (each chunk's pair on one worker)" if args.e2e_mode == "roundtrip"
-                               else "xnyz_batch_compress then xnyz_batch_decompress"),
-                "parallelism": f"replicas x{world}",
+            "config": workload_config(args.workload, n, variants, world),
+            "paths": {
+                "value": f"device-resident points and pre-zstd container; the independent variants spread "
+                         f"over {pipes} contexts / streams, CUDA events on the main stream bracketing all",
+                "e2e": "pinned host points -> zstd frames (libzstd 1.5.7 level 3) -> pinned host points, "
+                       + ("xnyz_batch_roundtrip (each chunk's pair on one worker)" if args.e2e_mode == "roundtrip"
+                          else "xnyz_batch_compress then xnyz_batch_decompress"),
             },
             "bits_per_point": bpp,
             "e2e": ({"value": round(e2e, 4), "unit": "GB/s", "h2d_bytes_per_step": int(12 * n * len(variants)),
@@ -445,6 +478,9 @@ def run_gpu(args):
             "gpu_launches": int(launches),
             "clocks": clk,
         }
+        if parity is not None:
+            line["parity"] = parity.pop("per_variant")
+            line["parity_detail"] = parity
         if learned is not None:
             line["learned"] = learned
         if batched is not None:
@@ -458,6 +494,66 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- parity ---
+def parity_measure(ctx, dev, d_pts, host, n, variants, workload, seed, mono_frames, mono_outs):
+    """The timed paths' outputs against the reference's, at full size, after the timed region.
+
+    Per variant: the device container (xnyz_compress_device), the zstd frame of the
+    host-output call (xnyz_compress from the resident points), the device decode
+    (xnyz_decompress_device), and the last e2e step's whole-cloud frame and host points, each
+    by SHA-256 against tests/golden/ref_digests.json (the reference run on the same seeded
+    cloud); and the L2 report of xnyzip_b200.verify (every input point against its cell's
+    recovered point, the decoded cloud against those points)."""
+    import numpy as np
+    import torch
+    from xnyzip_b200 import verify as V
+    key = f"{workload}_{n}_seed{seed}"
+    ref = load_digests().get(key)
+    t0 = time.time()
+    out = {"reference_digests": key if ref else None}
+    if ref:
+        out["input_matches_reference_input"] = V.sha256(host) == ref["input_sha256"]
+    per, l2rep = {}, {}
+    pts = d_pts.view(n, 3)
+    for v in variants:
+        q, l2, hil, rle = v
+        name = vname(v)
+        p, ln = ctx.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
+        torch.cuda.current_stream(dev).synchronize()
+        got = {"container": V.sha256(V.device_view(p, (ln,), "|u1", dev))}
+        dp, nout = ctx.decompress_device(p, ln, q, l2, rle)
+        torch.cuda.current_stream(dev).synchronize()
+        dec = V.device_view(dp, (nout, 3), "<f4", dev).clone()  # the context reuses its output buffer
+        got["points"] = V.sha256(dec)
+        got["frame"] = V.sha256(ctx.compress(d_pts, q, l2, hil, rle))
+        if mono_frames is not None and v in mono_frames:
+            got["e2e_frame"] = V.sha256(np.asarray(mono_frames[v]).tobytes())
+            got["e2e_points"] = V.sha256(mono_outs[variants.index(v)])
+        l2rep[name] = V.l2_report(ctx, pts, q, l2, decoded=dec)
+        del dec
+        if ref and name in ref["variants"]:
+            r = ref["variants"][name]
+            want = {"container": r["container_sha256"], "points": r["points_sha256"], "frame": r["frame_sha256"],
+                    "e2e_frame": r["frame_sha256"], "e2e_points": r["points_sha256"]}
+            checks = {k: got[k] == want[k] for k in got}
+            per[name] = all(checks.values())
+            if not per[name]:
+                out.setdefault("failed_checks", {})[name] = [k for k, ok in checks.items() if not ok]
+        else:
+            per[name] = None
+    torch.cuda.empty_cache()
+    out["per_variant"] = per
+    out["checked"] = ["container", "frame", "points", "e2e_frame", "e2e_points"] if mono_frames else \
+        ["container", "frame", "points"]
+    out["all_identical"] = bool(per) and all(x is True for x in per.values())
+    out["l2"] = l2rep
+    out["max_l2_error"] = max(r["max_l2_error"] for r in l2rep.values())
+    out["over_bound"] = sum(r["over_bound"] for r in l2rep.values())
+    out["decoded_mismatch_minus_z_minus1"] = sum(r["mismatch"] - r["z_minus1_points"] for r in l2rep.values())
+    out["check_s"] = round(time.time() - t0, 1)
+    return out
 
 
 # ------------------------------------------------------------- learned block parameters ---
@@ -706,7 +802,12 @@ def cpu_baseline(host, variants, sample_points, threads=1):
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU path on all host threads (per-chunk mode)."""
+    """--impl reference: the reference CPU path on all host threads, in its per-chunk mode.
+
+    The arm regenerates the bench's cloud (same generator, size and seed as the GPU arm's
+    rank 0) and each step has every host thread compress and decompress, in all variants,
+    its own --chunk-point chunk of it; the chunks are spread evenly over the cloud.  That is
+    a bounded sample of the GPU arm's workload, whose config the line repeats unchanged."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -714,15 +815,18 @@ def run_reference(args):
     lib, kind = _ref_lib()
     threads = os.cpu_count() or 1
     chunk = args.chunk
-    n_total = chunk * threads
-    host = make_cloud(args.workload, n_total, 1)
+    n = args.points or WORKLOADS[args.workload][1]
+    host = make_cloud(args.workload, n, cloud_seed(args.workload, 0))
+    stride = max(chunk, (n // threads) // chunk * chunk)
+    starts = [min(t * stride, max(0, n - chunk)) for t in range(threads)]
+    n_sample = sum(min(chunk, n - a) for a in starts)
     variants = WORKLOADS[args.workload][2][: args.variants]
     if kind == "reference":
         lib.quiet(True)
 
     def step():
         def work(t):
-            x = host[t * chunk:(t + 1) * chunk]
+            x = host[starts[t]:starts[t] + chunk]
             for q, l2, hil, rle in variants:
                 fr = lib.compress(x, QNAME[q], l2, hil, rle)
                 lib.decompress(fr, QNAME[q], l2, rle)
@@ -742,16 +846,16 @@ def run_reference(args):
     finally:
         if kind == "reference":
             lib.quiet(False)
-    value = 12.0 * n_total * len(variants) * args.steps / dt / 1e9
-    sample = (f"{threads} threads x {chunk}-point chunks of the {args.workload} cloud (the reference's per-chunk mode), "
-              f"all {len(variants)} variants per step")
+    value = 12.0 * n_sample * len(variants) * args.steps / dt / 1e9
+    sample = (f"{threads} host threads, each compressing and decompressing (all {len(variants)} variants, zstd "
+              f"frames) one {chunk}-point chunk of the {n}-point cloud per step, chunks spread evenly over it "
+              f"({n_sample} points per step; the reference's per-chunk mode)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {**workload_config(args.workload, args.points or WORKLOADS[args.workload][1], variants),
-                   "sample_points_per_step": n_total,
-                   "parallelism": f"{threads} host threads, one {chunk}-point chunk each (per-chunk mode)"},
+        "config": workload_config(args.workload, n, variants, world),
+        "sample": {"points_per_step": n_sample, "chunk_points": chunk, "threads": threads},
         "cpu_baseline": {"value": round(value, 5), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 5), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -781,6 +885,8 @@ def main():
                     help="frames of the GPU zstd decoding measurement (0: skip it)")
     ap.add_argument("--zstd-only", action="store_true",
                     help="run only the GPU zstd decoding measurement and print it")
+    ap.add_argument("--parity", action=argparse.BooleanOptionalAction, default=True,
+                    help="check the timed paths' outputs against the reference digests after the timed region")
     ap.add_argument("--learned", action=argparse.BooleanOptionalAction, default=True,
                     help="also measure the extended container with learned block parameters")
     args = ap.parse_args()

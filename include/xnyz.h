@@ -340,8 +340,9 @@ xnyz_status xnyz_batch_autotune(xnyz_batch* batch, uint64_t count, const float* 
  * optional uint32 payload) in place over bits [0, key_bits) on `stream` (a cudaStream_t, NULL
  * = default stream) on the current device, and waits for the result.  n > 2^20 returns
  * XNYZ_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address; make
- * it before any stream capture.  Calls share the array: calls that overlap on the GPU race,
- * so serialise them. */
+ * it before any stream capture.  That address is cached per device for the primary context:
+ * after cudaDeviceReset it is stale.  Calls share the array: calls that overlap on the GPU
+ * (two streams, two host threads) race, so serialise them. */
 xnyz_status xnyz_sort_noalloc(uint64_t* dev_keys, uint32_t* dev_payload, uint64_t n, int key_bits, void* stream);
 
 /* ---- profiling ---------------------------------------------------------------------------- */

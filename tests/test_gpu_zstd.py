@@ -112,6 +112,21 @@ def test_damaged_frames(ctx, xnyz):
     assert lens[0] == len(data) and outs[0] == data
 
 
+def test_too_many_huffman_weights(ctx, xnyz):
+    """A frame whose Huffman tree description codes 256 weights (one more than a tree can have)
+    fails with XNYZ_ERR_BAD_STREAM, beside a good frame; the context stays usable."""
+    from zstd_craft import frame_with_huf_tree, huf_tree_256_weights
+    z = _libzstd()
+    data = b"0123456789abcdef" * 500
+    f = _zstd(z, data, 3)
+    bad = frame_with_huf_tree(huf_tree_256_weights())
+    with pytest.raises(xnyz.XnyzError) as e:
+        _gpu_decode(ctx, [f, bad], [len(data), 256])
+    assert e.value.status == 2  # XNYZ_ERR_BAD_STREAM
+    lens, outs, _, _ = _gpu_decode(ctx, [f], [len(data)])
+    assert lens[0] == len(data) and outs[0] == data
+
+
 def test_random_frames(ctx):
     """48 seeded frames of mixed random, run, geometric and repeated data (up to ~1.5 MB, levels
     1-19), decoded in one call: every frame equals libzstd's input."""

@@ -141,6 +141,54 @@ def test_host_decoder_matches_libzstd(zd, team):
             assert out.raw[:len(d)] == d
 
 
+ASAN_MAIN = r"""
+#include "zstd_dec.cuh"
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+int main(int argc, char** argv) {
+    FILE* f = std::fopen(argv[1], "rb");
+    std::vector<unsigned char> s(1 << 16);
+    const size_t n = std::fread(s.data(), 1, s.size(), f);
+    std::fclose(f);
+    auto* ws = static_cast<xnyz::zd::Workspace*>(std::malloc(sizeof(xnyz::zd::Workspace)));
+    std::vector<unsigned char> d(4096);
+    const long long r = xnyz::zd::decode_frame(s.data(), n, d.data(), d.size(), *ws, xnyz::zd::SoloTeam{});
+    std::free(ws);
+    std::printf("%lld\n", r);
+    return 0;
+}
+"""
+
+
+def test_host_decoder_256_huffman_weights(tmp_path):
+    """A Huffman tree description whose FSE-coded weights run to 256 entries is refused with a
+    negative code, and (under AddressSanitizer) the decoder writes nothing past its weight
+    array; libzstd refuses the same frame."""
+    from zstd_craft import frame_with_huf_tree, huf_tree_256_weights
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("no host C++ compiler")
+    shutil.copy(HEADER, tmp_path / "zstd_dec.cuh")
+    (tmp_path / "m.cpp").write_text(ASAN_MAIN)
+    exe = tmp_path / "zd_asan"
+    subprocess.run([cxx, "-O1", "-g", "-std=c++20", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
+                    str(tmp_path / "m.cpp"), "-o", str(exe)], check=True)
+    frame = frame_with_huf_tree(huf_tree_256_weights())
+    (tmp_path / "f.bin").write_bytes(frame)
+    r = subprocess.run([str(exe), str(tmp_path / "f.bin")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert int(r.stdout.strip()) < 0
+    z = C.CDLL(__import__("xnyzip_b200._native", fromlist=["x"]).default_zstd_library())
+    z.ZSTD_decompress.restype = C.c_size_t
+    z.ZSTD_decompress.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]
+    z.ZSTD_isError.restype = C.c_uint
+    z.ZSTD_isError.argtypes = [C.c_size_t]
+    out = C.create_string_buffer(256)
+    assert z.ZSTD_isError(z.ZSTD_decompress(out, 256, frame, len(frame)))
+
+
 @pytest.mark.parametrize("team", ["zd_solo", "zd_team"])
 def test_host_decoder_damaged_frames(zd, team):
     frame = _zstd()

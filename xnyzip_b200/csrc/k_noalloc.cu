@@ -11,10 +11,12 @@
 // that loads this part of the library holds it until the process exits.  Host code cannot use
 // the array's name as a device address, so the first call on each device looks the address
 // up with cudaGetSymbolAddress (with that device current) and caches it; make that first call
-// before any stream capture.  All calls share the array and it keeps the last call's
-// contents: the digit histograms, tile counters and error word are cleared at the start of
-// every call, and the look-back words are epoch-tagged.  Calls that overlap on the GPU (two
-// streams, two host threads on one device) race on the array; serialise them.
+// before any stream capture.  The cached address belongs to the device's primary context: after
+// cudaDeviceReset it is stale, so do not call this entry point again in that process.  All
+// calls share the array and it keeps the last call's contents: the digit histograms, tile
+// counters and error word are cleared at the start of every call, and the look-back words are
+// epoch-tagged.  Calls that overlap on the GPU (two streams, two host threads on one device)
+// race on the array; serialise them.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -69,6 +71,7 @@ extern "C" xnyz_status xnyz_sort_noalloc(uint64_t* dev_keys, uint32_t* dev_paylo
     if (key_bits < 0 || key_bits > 64) return XNYZ_ERR_INVALID_ARG;
     const int passes = (key_bits + 7) / 8;
     if (n <= 1 || passes == 0) return XNYZ_OK;
+    (void)cudaGetLastError();  // an earlier launch's error on this thread is not this call's failure
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return XNYZ_ERR_CUDA;
     unsigned char* s = nullptr;
@@ -104,6 +107,7 @@ extern "C" xnyz_status xnyz_sort_noalloc(uint64_t* dev_keys, uint32_t* dev_paylo
                          counters + p, err, st);
         cur ^= 1;
     }
+    if (cudaGetLastError() != cudaSuccess) return XNYZ_ERR_CUDA;  // a launch was refused
     if (cur) {  // result in the scratch copy: back into the caller's arrays
         if (cudaMemcpyAsync(dev_keys, keys_alt, 8 * n, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return XNYZ_ERR_CUDA;
         if (dev_payload &&

@@ -340,6 +340,7 @@ ZD_HD int read_huf_tree(const u8* src, u64 len, Workspace& ws, int& huf_bits, co
     if (maxb > kHufMaxBits) return kErrFormat;
     const u32 rest = (1u << maxb) - sum;
     if (rest & (rest - 1)) return kErrFormat;
+    if (nw > 255) return kErrFormat;  // 255 explicit weights at most: the implied one is the 256th
     w[nw++] = (u8)(highbit(rest) + 1);
     // codes in order of increasing weight, then symbol; weight w spans 2^(w-1) entries
     u32 start[kHufMaxBits + 2] = {};
