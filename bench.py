@@ -392,6 +392,7 @@ def run_gpu(args):
     learned = None
     if args.learned and rank == 0:
         learned = learned_measure(ctx, stream, d_pts, n, variants, args.steps)
+        learned["mlp_kernels"] = mlp_measure(dev, stream)
 
     # ---- the uneven batch (2048 clouds): per-cloud plain launches vs the batched path ----
     batched = None
@@ -561,7 +562,8 @@ def learned_measure(ctx, stream, d_pts, n, variants, steps):
     """Extended container on the resident cloud: pre-zstd bits/point of the repos /
     SFC-delta stream's coding under each block mode (reference Huffman+GR container, one
     global parameter pair, the learned predictor, exhaustive search) and the device
-    compress+decompress GB/s of the learned path against the plain path."""
+    compress+decompress GB/s of each: the plain path (reference container), the learned
+    predictor, the exhaustive per-block search it stands in for, and one global pair."""
     import torch
     import xnyzip_b200 as X
     modes = {"reference": 0, "global": 3, "learned": 2, "exhaustive": 1}
@@ -596,7 +598,7 @@ def learned_measure(ctx, stream, d_pts, n, variants, steps):
                 raise RuntimeError("learned round trip lost points")
 
     rates = {}
-    for name, m in (("plain", 0), ("learned", 2)):
+    for name, m in (("plain", 0), ("learned", 2), ("exhaustive", 1), ("global", 3)):
         step(m)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -609,8 +611,73 @@ def learned_measure(ctx, stream, d_pts, n, variants, steps):
     ctx.set_block_mode(0)
     out["device_GB_s"] = {k: round(v, 3) for k, v in rates.items()}
     out["speedup_vs_plain"] = round(rates["learned"] / rates["plain"], 4)
+    out["speedup_vs_exhaustive"] = round(rates["learned"] / rates["exhaustive"], 4)
     out["note"] = ("extended container: the repos / SFC-delta stream in 1024-value blocks with per-block PFor "
                    "width and Golomb-Rice k; other streams as in the reference container; pre-zstd sizes")
+    return out
+
+
+# ------------------------------------------------------------------ the predictor's MLP ---
+def mlp_measure(dev, stream, blocks=1 << 20, reps=10):
+    """The block-parameter predictor's kernels alone: inference (xnyz_mlp_forward) and one
+    training step's forward + backward (xnyz_mlp_train_batch) over `blocks` blocks of random
+    features, CUDA events on `stream`, best of `reps`.  FLOPs per block: 2 * (34*64 + 64*64 +
+    64*65) = 20,864 for inference (the dense layers), three times that for training (forward,
+    dX and dW); reported against the measured dense bf16 peak as tensor-pipe context: the
+    layers are 34-65 wide, far from a GEMM's shape."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from xnyzip_b200 import _native as N
+    prm_host = np.fromfile(os.path.join(ROOT, "xnyzip_b200", "model", "blockparams.f32"), dtype=np.float32)
+    prm = torch.from_numpy(prm_host).to(dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    feats = torch.rand((blocks, 34), generator=g, device=dev, dtype=torch.float32)
+    feats[:, :32] /= feats[:, :32].sum(dim=1, keepdim=True)
+    w = torch.randint(0, 33, (blocks,), generator=g, device=dev, dtype=torch.uint8)
+    k = torch.randint(0, 32, (blocks,), generator=g, device=dev, dtype=torch.uint8)
+    pw = torch.empty(blocks, dtype=torch.uint8, device=dev)
+    pk = torch.empty_like(pw)
+    grad = torch.zeros_like(prm)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    gather = torch.empty(N.mlp_gather_floats(blocks), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize(dev)
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    st = C.c_void_p(stream.cuda_stream)
+
+    def fwd():
+        N.check(N.mlp_forward(p(prm), p(feats), blocks, p(pw), p(pk), None, None, st))
+
+    def train():
+        N.check(N.mlp_train_batch(p(prm), p(feats), p(w), p(k), None, 0, blocks, 1.0 / blocks, p(grad), p(loss),
+                                  p(gather), st))
+
+    out = {}
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak = 1590.0
+    for name, fn, flops in (("inference", fwd, 20864.0), ("training_step", train, 3 * 20864.0)):
+        fn()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        t = min(ts)
+        tf = flops * blocks / t / 1e12
+        out[name] = {"ms": round(t * 1e3, 4), "blocks_per_s": round(blocks / t, 1), "TFLOP_s": round(tf, 3),
+                     "frac_of_bf16_peak": round(tf / peak, 5)}
+    out["blocks"] = blocks
+    out["note"] = ("34-64-64-65 MLP, BF16 operands / FP32 accumulation on mma.sync m16n8k16; one inference "
+                   "block = 1024 values of the repos / SFC-delta stream")
+    del feats, grad, gather
     return out
 
 
@@ -641,7 +708,7 @@ def batched_measure(ctx, stream, dev, count, workers):
             if nout != n:
                 raise RuntimeError("plain round trip lost points")
 
-    rep_s = {}
+    rep_s, med_s = {}, {}
 
     def timed(fn, name, reps=3):
         """Best of `reps` timed runs after one warm-up (a run that grows a worker's workspace
@@ -655,6 +722,7 @@ def batched_measure(ctx, stream, dev, count, workers):
             torch.cuda.synchronize(dev)
             ts.append(time.perf_counter() - t)
         rep_s[name] = [round(x, 4) for x in ts]
+        med_s[name] = statistics.median(ts)
         return min(ts)
 
     ctx.set_block_mode(0)
@@ -680,6 +748,8 @@ def batched_measure(ctx, stream, dev, count, workers):
     out["points_per_s"] = {k: round(total / v, 1) for k, v in res.items()}
     out["GB_s"] = {k: round(12.0 * total / v / 1e9, 3) for k, v in res.items()}
     out["speedup_vs_plain"] = {k: round(res["plain"] / v, 3) for k, v in res.items() if k != "plain"}
+    out["GB_s_median"] = {k: round(12.0 * total / v / 1e9, 3) for k, v in med_s.items()}
+    out["speedup_vs_plain_median"] = {k: round(med_s["plain"] / v, 3) for k, v in med_s.items() if k != "plain"}
     out["note"] = ("compress+decompress of every cloud, device-resident; size classes by point count "
                    "(powers of four from 16K), concurrent worker streams per class from the autotuner")
     del clouds
@@ -883,6 +953,8 @@ def main():
                     help="clouds of the uneven batch workload (0: skip that measurement)")
     ap.add_argument("--zstd-frames", type=int, default=6360,
                     help="frames of the GPU zstd decoding measurement (0: skip it)")
+    ap.add_argument("--mlp-only", action="store_true",
+                    help="run only the predictor's kernel measurement (inference and training) and print it")
     ap.add_argument("--zstd-only", action="store_true",
                     help="run only the GPU zstd decoding measurement and print it")
     ap.add_argument("--parity", action=argparse.BooleanOptionalAction, default=True,
@@ -894,6 +966,10 @@ def main():
         log("warning: fewer than 3 warm-up steps")
     if args.impl == "reference":
         run_reference(args)
+    elif args.mlp_only:
+        import torch
+        stream = torch.cuda.Stream()
+        print(json.dumps({"mlp_kernels": mlp_measure(torch.device("cuda", 0), stream)}), flush=True)
     elif args.zstd_only:
         import torch
         import xnyzip_b200 as X
