@@ -78,7 +78,10 @@ def test_cli_matches_reference(inputs, case):
         q = mode[0]
         eo = np.fromfile(wo / f"errors-{q}.bin", np.float32)
         er = np.fromfile(wr / f"errors-{q}.bin", np.float32)
-        # position by position, up to points of one lattice cell taken in another order
+        # position by position, up to points of one lattice cell taken in another order: where
+        # the errors differ, the decoded point is that of a run of one cell
         assert eo.shape == er.shape and np.array_equal(np.sort(eo), np.sort(er))
-        assert np.mean(eo == er) > 0.999
+        dec = np.fromfile(wo / "decomp.bin", np.float32).reshape(-1, 3)
+        for i in np.flatnonzero(eo != er):
+            assert (dec[i] == dec[max(i - 1, 0)]).all() or (dec[i] == dec[min(i + 1, len(dec) - 1)]).all(), i
     assert any(re.match(r"chunk compressed bytes:\s*(\d+)", ln) for ln in lr)

@@ -3,11 +3,10 @@ generator, seed 1) in all six variants of the bench (TO and cube x L2 {0.001, 0.
 Hilbert, -rle), through the device path and the host-buffer path, compared by SHA-256 with
 what the reference itself produced on the same cloud (tests/golden/ref_digests.json, made by
 tests/golden/make_ref_digests.py): the pre-zstd container, the zstd frame and the decoded
-points, plus the L2 bound of every point."""
+points, plus the L2 bound of every point (up to float32 resolution, xnyzip_b200.verify)."""
 import json
 import os
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -51,7 +50,9 @@ def test_terrain_8m_matches_reference(ctx, cloud, q, l2):
     assert len(frame) == want["frame_bytes"] and V.sha256(frame) == want["frame_sha256"]
     back = ctx.decompress(frame, q, l2, True)
     assert V.sha256(back) == want["points_sha256"]
+    # every point within its bound up to the float32 resolution of the reference's arithmetic
+    # on a 10 km cloud (a 1 mm bound is below it: the reference's own decoded points, which
+    # these are, exceed 1 mm for many points)
     rep = V.l2_report(ctx, d, q, l2, decoded=dec)
-    assert rep["over_bound"] == 0, rep
-    assert rep["max_l2_error"] <= np.float32(l2)
+    assert rep["over_bound_plus_slack"] == 0, rep
     assert rep["mismatch"] == rep["z_minus1_points"], rep

@@ -12,6 +12,13 @@ These checks work for both container kinds:
 * the decoded cloud must be the multiset {r_i} (a -normal container reorders the points,
   a -rle container repeats each cell's point by its count), compared through a 64-bit hash
   of each point's bits;
+* float32 resolution: the reference quantizes and recovers in float32, so on a cloud whose
+  extent E is large against the bound the lattice index p / step is itself rounded (its
+  spacing is ulp(E / step) steps) and so are the shift (ulp(E)) and the unshift (ulp(M), M the
+  largest coordinate).  The report gives that slack, sqrt(3) * (step * ulp(E / step) + ulp(E)
+  + ulp(M)), and counts the points beyond
+  bound + slack, which must be none; points between the bound and bound + slack are the
+  reference's own (its decoded points are these, bit for bit);
 * points whose truncated-octahedron cell has z = -1 (a point on the bottom face of the
   bounding box, where round(-0.5) = -1) are counted apart: the reference's block arithmetic
   wraps their block id and decodes them far away, and this path reproduces that.
@@ -90,14 +97,35 @@ def multiset_mismatch(a, b) -> int:
     return int(a.shape[0] - torch.minimum(ca, cb).sum().item())
 
 
+def _ulp32(x: float) -> float:
+    """Spacing of float32 values at magnitude x."""
+    x = abs(float(np.float32(x)))
+    return float(np.spacing(np.float32(x))) if x > 0 else float(np.finfo(np.float32).tiny)
+
+
+def f32_slack(points, quantizer: int, l2: float) -> float:
+    """Float32 resolution of the reference's arithmetic on this cloud (see the module text):
+    sqrt(3) * (step * ulp(E / step) + ulp(E) + ulp(M)), E the largest per-axis extent, M the
+    largest coordinate magnitude, step the
+    quantizer's lattice step (2 l2 / sqrt(5) for the truncated octahedron, 2 l2 / sqrt(3) for
+    the cube)."""
+    if points.shape[0] == 0:
+        return 0.0
+    ext = float((points.max(dim=0).values - points.min(dim=0).values).max().item())
+    big = float(points.abs().max().item())
+    step = float(np.float32(2.0 * np.float32(l2) / np.sqrt(5.0 if quantizer == 1 else 3.0)))
+    return float(np.sqrt(3.0) * (step * _ulp32(ext / step) + _ulp32(ext) + _ulp32(big)))
+
+
 def l2_report(ctx, points, quantizer: int, l2: float, decoded=None) -> dict:
     """Error of every input point against its cell's recovered point, and (with `decoded`, an
     (m, 3) float32 device tensor) how the decoded cloud matches those points.
 
     points: (n, 3) float32 CUDA tensor.  Returns max_l2_error, over_bound (float compare, as
-    main.cpp), z_minus1_points, and with `decoded`: decoded_points and mismatch (decoded points
-    without an equal recovered input point; equal to z_minus1_points in a -rle or -normal
-    container of the truncated octahedron, whose wrapped cells decode elsewhere)."""
+    main.cpp), f32_slack and over_bound_plus_slack, z_minus1_points, and with `decoded`:
+    decoded_points and mismatch (decoded points without an equal recovered input point; equal
+    to z_minus1_points in a -rle or -normal container of the truncated octahedron, whose
+    wrapped cells decode elsewhere)."""
     import torch
     n = points.shape[0]
     cells = torch.empty((n, 3), dtype=torch.int32, device=points.device)
@@ -111,8 +139,11 @@ def l2_report(ctx, points, quantizer: int, l2: float, decoded=None) -> dict:
     d = points - rec
     sq = d * d
     err = torch.sqrt(sq[:, 0] + (sq[:, 1] + sq[:, 2]))
+    slack = f32_slack(points, quantizer, l2)
     out = {"max_l2_error": float(err.max().item()) if n else 0.0,
            "over_bound": int((err > l2).sum().item()),
+           "f32_slack": slack,
+           "over_bound_plus_slack": int((err.double() > l2 + slack).sum().item()),
            "z_minus1_points": int((cells[:, 2] == -1).sum().item()) if quantizer == 1 else 0}
     del cells, err, sq, d
     if decoded is not None:
