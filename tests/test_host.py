@@ -92,3 +92,51 @@ def test_count_stream_codebook_matches_oracle_container(xnyz, oracle):
         # The exp-Golomb decision depends on the count multiset only, not on its order.
         _, _, eg = _codebook(reps, 2, count_stream=True)
         assert (b"\xe1\xc1\x01\x01" in raw) == eg
+
+
+UDIV_CHECK = r"""
+#include "kernels.h"
+#include <cstdio>
+#include <random>
+using u64 = unsigned long long;
+// the device formula of k_decode.cu's udiv, with a 128-bit product for mulhi
+static u64 udiv(u64 x, const xnyz::dev::U64Div& d) {
+    const u64 t = (u64)(((unsigned __int128)d.m * x) >> 64);
+    return (t + ((x - t) >> d.sh1)) >> d.sh2;
+}
+int main() {
+    std::mt19937_64 rng(7);
+    u64 ds[] = {1, 2, 3, 5, 7, 64, 127, 128, 129, 1000, 78126, (1ull << 21) + 1, (1ull << 31) - 1, 1ull << 31,
+                (1ull << 32) - 5, 0xffffffffull, 1ull << 40, (1ull << 63) + 3, ~0ull};
+    long bad = 0, checks = 0;
+    for (u64 d : ds) {
+        const auto m = xnyz::dev::make_u64div(d);
+        u64 xs[] = {0, 1, d - 1, d, d + 1, 2 * d - 1, ~0ull, ~0ull - 1, 1ull << 63, (1ull << 58) * 3 + 11};
+        for (u64 x : xs) { ++checks; if (udiv(x, m) != x / d) ++bad; }
+        for (int i = 0; i < 200000; ++i) {
+            const u64 x = rng() >> (rng() % 64);
+            ++checks;
+            if (udiv(x, m) != x / d) ++bad;
+        }
+    }
+    std::printf("%ld %ld\n", checks, bad);
+    return bad != 0;
+}
+"""
+
+
+def test_invariant_divisor_multiply(tmp_path):
+    """The block-coordinate division of recover_units (x / nx, x / ny for any u64 block id,
+    wrapped ids of the z = -1 cells included) by a precomputed multiplier equals x / d."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "udiv.cpp"
+    src.write_text(UDIV_CHECK)
+    exe = tmp_path / "udiv"
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "xnyzip_b200", "csrc")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", csrc, str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout

@@ -1257,6 +1257,7 @@ struct DecodeJob {
     int slot = 0;
     bool fill = false;
     uint64_t fill_value = 0;
+    int fixed_len = 0;  // Huffman: every codeword has this length (decoded without entry tables)
 };
 
 // cells_out: decompress_to_cells (block_decompressor_rle.hpp:230-335): *d_out receives the
@@ -1437,6 +1438,9 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         j.table.symvals = t.direct_values ? nullptr : at<unsigned long long>(c, o.sym);
         j.table.root_bits = t.root_bits;
         j.L = std::max(1, t.max_len);
+        bool same = !pm.codes.empty();
+        for (const auto& ce : pm.codes) same = same && ce.len == t.max_len;
+        if (same && t.max_len == t.root_bits) j.fixed_len = t.max_len;
         jobs.push_back(j);
         return XNYZ_OK;
     };
@@ -1500,6 +1504,13 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         cudaStream_t js = side(c, j.slot);
         Prof pr(c, j.kind == kCodeGolombRice ? "decode_golomb_rice" : (j.kind == kCodeHuffman ? "decode_huffman" : "decode_exp_golomb"),
                 1, j.total_bits / 8.0 + static_cast<double>(j.nsym) * j.width, js);
+        if (j.fixed_len) {
+            if (j.nsym * static_cast<uint64_t>(j.fixed_len) > j.total_bits)
+                return fail(XNYZ_ERR_BAD_STREAM, "Huffman stream shorter than its symbols");
+            launch_decode_fixed(j.words, j.base_bits, j.total_bits, j.table, j.fixed_len, j.nsym, j.width, j.out,
+                                SMALL_FIELD(c, err), js);
+            continue;
+        }
         // Golomb-Rice tracks k + 2 entry offsets per subsequence (derived in the kernel).
         const uint32_t* Lrun = nullptr;
         CUDA_TRY(cudaMemsetAsync(at<uint32_t>(c, o_dflag[j.slot]), 0, 4 * dtiles, js));
@@ -1518,7 +1529,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(fetch_small(c, offsetof(Small, fallback), sizeof(uint32_t) * 8));
     bool refetch = false;
     for (auto& j : jobs) {
-        if (j.fill) continue;
+        if (j.fill || j.fixed_len) continue;
         if (c->h_small->fallback[j.slot]) {
             launch_decode_sequential(j.kind, j.words, j.base_bits, j.total_bits, j.table, j.nsym, j.width, j.out,
                                      SMALL_FIELD(c, codewords[j.slot]), SMALL_FIELD(c, err), st);
@@ -1534,7 +1545,7 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(fetch_small(c, offsetof(Small, totals), offsetof(Small, tile_counters) - offsetof(Small, totals)));
     TRY(check_device_errors(c));
     for (auto& j : jobs)
-        if (!j.fill && c->h_small->codewords[j.slot] < j.nsym)
+        if (!j.fill && !j.fixed_len && c->h_small->codewords[j.slot] < j.nsym)
             return fail(XNYZ_ERR_BAD_STREAM, "stream " + std::to_string(j.slot) + " holds " +
                                                  std::to_string(c->h_small->codewords[j.slot]) + " codes, expected " +
                                                  std::to_string(j.nsym));
@@ -1559,6 +1570,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     // nx uses the size_t conversion of the stored int range (block_quantizer.hpp:163)
     rp.nx = static_cast<uint64_t>(static_cast<int64_t>(h.rx)) / 128 + 1;
     rp.ny = static_cast<uint64_t>(static_cast<int64_t>(h.ry)) / 128 + 1;
+    rp.div_nx = make_u64div(rp.nx);
+    rp.div_ny = make_u64div(rp.ny);
     rp.hilbert = h.hilbert;
     rp.hstart_inv = hm.inv_block_start;
     rp.rle = rle && !cells_out;

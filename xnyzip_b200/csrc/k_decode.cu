@@ -19,6 +19,12 @@ constexpr int kItems = 16;
 constexpr int kTile = kThreads * kItems;
 static_assert(kTile == kScanTile, "tile size");
 
+// x / d for an invariant divisor (U64Div, kernels.h)
+__device__ __forceinline__ u64 udiv(u64 x, const U64Div& d) {
+    const u64 t = __umul64hi(d.m, x);
+    return (t + ((x - t) >> d.sh1)) >> d.sh2;
+}
+
 // ------------------------------------------------------------------ bit unpack ----------
 __global__ void __launch_bounds__(kThreads) bitunpack_kernel(const u32* __restrict__ words, u64 base, u64 n,
                                                              int width, u64* __restrict__ vals) {
@@ -460,8 +466,9 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
             if (valid) {
                 if (qd == 0) atomicOr(a.err, kErrBadStream);  // quad patches never occur
                 const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
-                const u64 nx = a.rp.nx, ny = a.rp.ny;
-                const u64 pbx = (blk % nx * 2) * 64, pby = (blk / nx % ny * 2) * 64, pbz = (blk / nx / ny * 2) * 64;
+                // (blk % nx) * 128, (blk / nx % ny) * 128, (blk / nx / ny) * 128, u64 arithmetic
+                const u64 q1 = udiv(blk, a.rp.div_nx), q2 = udiv(q1, a.rp.div_ny);
+                const u64 pbx = (blk - q1 * a.rp.nx) * 128, pby = (q1 - q2 * a.rp.ny) * 128, pbz = q2 * 128;
                 u64 m = reposj;
                 if (a.rp.hilbert)
                     m = reposj < (1ull << 18) ? hilbert_apply(htab, reposj, 5, a.rp.hstart_inv)

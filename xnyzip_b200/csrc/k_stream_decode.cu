@@ -873,6 +873,51 @@ __global__ void decode_sequential_kernel(Args a) {
     *a.total_codewords = i;
 }
 
+// A Huffman stream whose codewords all have one length `len` (<= kMaxRootBits): symbol i is
+// bits [i len, (i + 1) len) of the stream, one primary-table lookup each, so the stream needs
+// neither entry tables nor look-back.  Thread g decodes symbols 4g .. 4g + 3 from one 64-bit
+// window (4 len <= 44 bits) and stores u8 symbols four at a time.  A chunk that is no
+// codeword sets kErrBadStream, as the chained decoder does.
+__global__ void __launch_bounds__(256) decode_fixed_kernel(const u32* __restrict__ words, u32 base, u64 nwords,
+                                                           int len, const u32* __restrict__ root,
+                                                           const u64* __restrict__ symvals, u64 nsym, int width,
+                                                           void* out, bool packed_ok, u32* err) {
+    const u64 groups = (nsym + 3) / 4;
+    auto wbe = [&](u64 k) -> u64 { return k < nwords ? (u64)__byte_perm(__ldg(words + k), 0, 0x0123) : 0ull; };
+    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (u64)gridDim.x * blockDim.x) {
+        const u64 i0 = 4 * g;
+        const int cnt = (int)min((u64)4, nsym - i0);
+        const u64 q = (u64)base + i0 * (u64)len;
+        const u64 k = q >> 5;
+        const u32 o = (u32)(q & 31u);
+        u64 win = ((wbe(k) << 32) | wbe(k + 1)) << o;
+        if (o) win |= wbe(k + 2) >> (32u - o);
+        bool bad = false;
+        u32 packed = 0;
+        for (int j = 0; j < cnt; ++j) {
+            const u32 code = (u32)(win >> (64 - len));
+            win <<= len;
+            const u32 e = __ldg(root + code);
+            if ((e >> 24) != (u32)len) bad = true;
+            const u64 val = symvals ? __ldg(symvals + (e & 0xffffffu)) : (u64)(e & 0xffffffu);
+            if (width == 1) {
+                packed |= ((u32)val & 0xffu) << (8 * j);
+            } else {
+                reinterpret_cast<u32*>(out)[i0 + j] = (u32)val;
+            }
+        }
+        if (width == 1) {
+            u8* o8 = reinterpret_cast<u8*>(out) + i0;
+            if (cnt == 4 && packed_ok) {
+                *reinterpret_cast<u32*>(o8) = packed;
+            } else {
+                for (int j = 0; j < cnt; ++j) o8[j] = (u8)(packed >> (8 * j));
+            }
+        }
+        if (bad) atomicOr(err, kErrBadStream);
+    }
+}
+
 __global__ void flag_error_kernel(u32* err) { atomicOr(err, kErrBadStream); }
 void atomic_flag_host_error(u32* err, cudaStream_t st) { flag_error_kernel<<<1, 1, 0, st>>>(err); }
 
@@ -938,6 +983,22 @@ void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, u
                              smem_max);
         decode_stream_kernel<kCodeExpGolomb><<<tiles, T, smem, st>>>(a);
     }
+}
+
+void launch_decode_fixed(const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t, int len,
+                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st) {
+    if (!nsym) return;
+    if (len < 1 || len > kMaxRootBits || len != t.root_bits || (out_width != 1 && out_width != 4) ||
+        nsym * (uint64_t)len > total_bits) {
+        atomic_flag_host_error(err, st);  // the host only routes complete fixed-length streams here
+        return;
+    }
+    const u64 nwords = (base_bits + total_bits + 31) / 32;
+    u64 blocks = (nsym / 4 + 256) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    const bool packed_ok = (reinterpret_cast<uintptr_t>(out) & 3u) == 0;
+    decode_fixed_kernel<<<(unsigned)blocks, 256, 0, st>>>(words, (u32)base_bits, nwords, len, t.root, t.symvals, nsym,
+                                                          out_width, out, packed_ok, err);
 }
 
 void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,

@@ -203,6 +203,10 @@ void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, u
                           unsigned long long* agg, unsigned long long* inc, uint32_t* tile_counter, uint32_t* err,
                           uint32_t* need_fallback, unsigned long long* total_codewords, cudaStream_t st);
 // One-thread decoder the host runs when a bounded wait of the parallel decoder expired.
+// A Huffman stream whose codewords all have length len (== t.root_bits <= 11): every symbol
+// from its own len bits (out_width 1: u8, 4: u32 values).
+void launch_decode_fixed(const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t, int len,
+                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st);
 void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,
                               DecodeTable t, uint64_t nsym, int out_width, void* out,
                               unsigned long long* total_codewords, uint32_t* err, cudaStream_t st);
@@ -211,12 +215,33 @@ void launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cu
 void launch_fill_u8(uint8_t* p, uint64_t n, uint8_t v, cudaStream_t st);
 void launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st);
 
+// Division of any 64-bit value by an invariant divisor d >= 1 through one high multiply
+// (T. Granlund and P. Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994, section 4, figure 4.1): with l = ceil(log2 d) and m = floor(2^64 (2^l - d) / d)
+// + 1, x / d = (t + ((x - t) >> min(l, 1))) >> max(l - 1, 0) where t = mulhi(m, x).
+struct U64Div {
+    unsigned long long m;
+    unsigned int sh1, sh2;
+};
+inline U64Div make_u64div(unsigned long long d) {
+    unsigned int l = 0;
+    while (l < 64 && (static_cast<unsigned __int128>(1) << l) < d) ++l;
+    const unsigned __int128 num = (static_cast<unsigned __int128>(1) << 64) *
+                                  ((static_cast<unsigned __int128>(1) << l) - d);
+    U64Div r;
+    r.m = static_cast<unsigned long long>(num / d + 1);
+    r.sh1 = l < 1 ? l : 1;
+    r.sh2 = l > 1 ? l - 1 : 0;
+    return r;
+}
+
 // LCP recovery (block mode) or SFC prefix sum (direct mode) fused with the PFor decode,
 // -rle expansion, recover and unshift.
 struct RecoverParams {
     QuantParams q;
     float off[3];
     unsigned long long nx, ny;
+    U64Div div_nx, div_ny;   // make_u64div(nx), make_u64div(ny)
     int hilbert;
     unsigned int hstart_inv;  // inverse-Hilbert state after levels 20..6 of zero digits
     int rle;
