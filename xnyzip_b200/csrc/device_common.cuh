@@ -491,6 +491,125 @@ __device__ __forceinline__ void warp_write_msb(u32* words, u64 pos, u64 val, u32
     if (__any_sync(kFullMask, act && w2 != 0u)) warp_or_word(words, k0 + 2, __byte_perm(w2, 0, 0x0123), act);
 }
 
+// One thread's run of consecutive codes of an MSB-first stream, from stream bit `pos` on
+// (begin / put / end).  Bits collect in a 64-bit buffer and leave a word at a time: the
+// run's first and last words may be shared with the neighbouring runs and are OR-ed in
+// atomically, the words in between belong to this run alone and are stored.  For short codes
+// this is one or two memory operations per run instead of one per code.
+struct MsbRun {
+    u32* words;
+    u64 k;    // word that buf's first bit belongs to
+    u64 buf;  // pending bits, first in bit 63
+    u32 nb;   // pending bits (< 32 between puts)
+    bool first;
+    __device__ __forceinline__ void begin(u32* w, u64 pos) {
+        words = w;
+        k = pos >> 5;
+        nb = (u32)(pos & 31u);  // the word's leading bits belong to the previous run: zeros here
+        buf = 0;
+        first = true;
+    }
+    __device__ __forceinline__ void flush() {
+        const u32 wv = __byte_perm((u32)(buf >> 32), 0, 0x0123);
+        if (first) {
+            if (wv) atomicOr(&words[k], wv);
+            first = false;
+        } else {
+            words[k] = wv;
+        }
+        buf <<= 32;
+        nb -= 32;
+        ++k;
+    }
+    // the low n (<= 32) bits of v, most significant first
+    __device__ __forceinline__ void put32(u32 v, u32 n) {
+        if (!n) return;
+        if (nb >= 32) flush();
+        buf |= ((u64)v << (64u - n)) >> nb;
+        nb += n;
+    }
+    __device__ __forceinline__ void zeros(u64 n) {
+        while (n) {
+            const u32 t = n > 32 ? 32u : (u32)n;
+            put32(0u, t);
+            n -= t;
+        }
+    }
+    // the low n (<= 64) bits of v, most significant first
+    __device__ __forceinline__ void put(u64 v, u32 n) {
+        if (n > 32) {
+            put32((u32)(v >> 32), n - 32);
+            put32((u32)v, 32);
+        } else {
+            put32((u32)v, n);
+        }
+    }
+    __device__ __forceinline__ void end() {
+        if (nb >= 32) flush();
+        if (nb) {  // the last word, shared with the next run
+            const u32 wv = __byte_perm((u32)(buf >> 32), 0, 0x0123);
+            if (wv) atomicOr(&words[k], wv);
+        }
+    }
+};
+
+// The LSB-first counterpart of MsbRun: bits collect from bit 0 of the buffer up.
+struct LsbRun {
+    u32* words;
+    u64 k;
+    u64 buf;  // pending bits, first in bit 0
+    u32 nb;
+    bool first;
+    __device__ __forceinline__ void begin(u32* w, u64 pos) {
+        words = w;
+        k = pos >> 5;
+        nb = (u32)(pos & 31u);
+        buf = 0;
+        first = true;
+    }
+    __device__ __forceinline__ void flush() {
+        const u32 wv = (u32)buf;
+        if (first) {
+            if (wv) atomicOr(&words[k], wv);
+            first = false;
+        } else {
+            words[k] = wv;
+        }
+        buf >>= 32;
+        nb -= 32;
+        ++k;
+    }
+    // the low n (<= 32) bits of v, least significant first
+    __device__ __forceinline__ void put32(u32 v, u32 n) {
+        if (!n) return;
+        if (nb >= 32) flush();
+        buf |= (u64)(n == 32u ? v : (v & ((1u << n) - 1u))) << nb;
+        nb += n;
+    }
+    __device__ __forceinline__ void ones(u64 n) {
+        while (n) {
+            const u32 t = n > 32 ? 32u : (u32)n;
+            put32(0xffffffffu, t);
+            n -= t;
+        }
+    }
+    __device__ __forceinline__ void put(u64 v, u32 n) {
+        if (n > 32) {
+            put32((u32)v, 32);
+            put32((u32)(v >> 32), n - 32);
+        } else {
+            put32((u32)v, n);
+        }
+    }
+    __device__ __forceinline__ void end() {
+        if (nb >= 32) flush();
+        if (nb) {
+            const u32 wv = (u32)buf;
+            if (wv) atomicOr(&words[k], wv);
+        }
+    }
+};
+
 // Writes `nbits` (<= 64) bits of `val`, least significant first, at position `pos` of an
 // LSB-first stream.
 __device__ __forceinline__ void warp_write_lsb(u32* words, u64 pos, u64 val, u32 nbits) {
