@@ -27,8 +27,9 @@ copies), Hilbert curve, -rle container, both quantizers (to, cube) x L2 bounds
           launches on one context against xnyz_batch_roundtrip_device (autotuned worker
           streams per size class), with the reference container and with learned parameters.
 
---workload spheres: the clustered-surface cloud instead (175M points on 200,000 spheres, TO,
-L2 0.5, Morton, -normal and -rle).
+spheres : the clustered-surface cloud (175M points on 200,000 spheres, TO, L2 0.5, Morton,
+          -normal and -rle), device GB/s and parity in its own sub-line (--no-spheres skips it);
+          --workload spheres makes it the main workload instead.
 
 --gpus N: one process per GPU (torchrun); the path does not shard, every rank runs its
 own replica on its own cloud (seed 1 + rank): weak scaling, max time over ranks.
@@ -399,6 +400,14 @@ def run_gpu(args):
     if args.batch_clouds and rank == 0 and world == 1:
         batched = batched_measure(ctx, stream, dev, args.batch_clouds, args.workers)
 
+    # ---- the clustered-surface cloud (175M points on 200,000 spheres), its own sub-line ----
+    spheres = None
+    if args.spheres and args.workload == "terrain" and rank == 0 and world == 1:
+        try:
+            spheres = spheres_measure(ctx, stream, dev, min(args.steps, 3), args.warmup, args.parity)
+        except Exception as e:  # reported in the line, the rest of it stands
+            spheres = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- zstd frames decoded on the GPU ----
     zstd_frames = None
     if args.zstd_frames and rank == 0 and world == 1:
@@ -486,6 +495,8 @@ def run_gpu(args):
             line["learned"] = learned
         if batched is not None:
             line["batched"] = batched
+        if spheres is not None:
+            line["spheres"] = spheres
         if zstd_frames is not None:
             line["zstd_frames"] = zstd_frames
         if cpu is not None:
@@ -495,6 +506,82 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# -------------------------------------------------------------------- spheres (config 3) ---
+def spheres_measure(ctx, stream, dev, steps, warmup, check_parity, n=175_000_000):
+    """The clustered-surface plain method (175M points on 200,000 spheres, TO, L2 0.5, Morton,
+    -normal and -rle): device-resident compress+decompress GB/s of both variants, each on its
+    own context and stream (CUDA events on `stream` bracket both), max-over-nothing (one
+    rank), and the same parity checks as the main workload against the reference's digests
+    of this cloud."""
+    import threading as th
+    import torch
+    import xnyzip_b200 as X
+    t0 = time.time()
+    host = make_cloud("spheres", n, cloud_seed("spheres", 0))
+    gen_s = time.time() - t0
+    d_pts = torch.from_numpy(host).to(dev)
+    torch.cuda.synchronize(dev)
+    variants = WORKLOADS["spheres"][2]
+    side = torch.cuda.Stream(dev)
+    ctx2 = X.Context(dev.index, stream=side.cuda_stream)
+    ctxs = [ctx, ctx2]
+    streams = [stream, side]
+
+    def one(c, v):
+        q, l2, hil, rle = v
+        p, ln = c.compress_device(d_pts.data_ptr(), n, q, l2, hil, rle)
+        _, nout = c.decompress_device(p, ln, q, l2, rle)
+        if nout != n:
+            raise RuntimeError(f"decoded {nout} points, expected {n}")
+
+    def step():
+        start = torch.cuda.Event()
+        start.record(stream)
+        side.wait_event(start)
+        errs = []
+
+        def work(i):
+            try:
+                one(ctxs[i], variants[i])
+            except Exception as e:  # re-raised below
+                errs.append(e)
+
+        ts = [th.Thread(target=work, args=(i,)) for i in range(2)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if errs:
+            raise errs[0]
+        done = torch.cuda.Event()
+        done.record(side)
+        stream.wait_event(done)
+
+    for _ in range(max(1, warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    ctx2.close()
+    out = {"workload": f"spheres {n} points on 200,000 spheres, TO, L2 0.5, Morton; one step = compress+decompress "
+                       "of the -normal and the -rle variant, one context / stream each",
+           "points": n, "variants": [vname(v) for v in variants], "steps": steps, "warmup": max(1, warmup),
+           "ms_per_step": round(ms, 3), "GB_s": round(12.0 * n * len(variants) / (ms / 1e3) / 1e9, 3),
+           "generate_s": round(gen_s, 1)}
+    if check_parity:
+        par = parity_measure(ctx, dev, d_pts, host, n, variants, "spheres", cloud_seed("spheres", 0), None, None)
+        out["parity"] = par.pop("per_variant")
+        out["parity_detail"] = par
+    del d_pts, host
+    torch.cuda.empty_cache()
+    return out
 
 
 # ----------------------------------------------------------------------------- parity ---
@@ -957,6 +1044,8 @@ def main():
                     help="run only the predictor's kernel measurement (inference and training) and print it")
     ap.add_argument("--zstd-only", action="store_true",
                     help="run only the GPU zstd decoding measurement and print it")
+    ap.add_argument("--spheres", action=argparse.BooleanOptionalAction, default=True,
+                    help="also measure the 175M-point spheres cloud (both variants, with parity) in its own sub-line")
     ap.add_argument("--parity", action=argparse.BooleanOptionalAction, default=True,
                     help="check the timed paths' outputs against the reference digests after the timed region")
     ap.add_argument("--learned", action=argparse.BooleanOptionalAction, default=True,
