@@ -275,13 +275,19 @@ xnyz_status join_sides(xnyz_ctx* c) {
     return XNYZ_OK;
 }
 
-xnyz_status check_device_errors(xnyz_ctx* c) {
-    TRY(fetch_small(c, offsetof(Small, err), sizeof(uint32_t)));
+// The device error word as last copied to the host.
+xnyz_status device_errors(xnyz_ctx* c) {
     const uint32_t e = c->h_small->err;
     if (e & 1u) return fail(XNYZ_ERR_TIMEOUT, "a bounded device wait expired");
     if (e & 2u) return fail(XNYZ_ERR_BAD_STREAM, "malformed bit stream");
     if (e & 4u) return fail(XNYZ_ERR_BAD_STREAM, "stream content exceeds its declared sizes");
+    if (e & 8u) return fail(XNYZ_ERR_TIMEOUT, "a scatter position fell outside its array after a wait expired");
     return XNYZ_OK;
+}
+
+xnyz_status check_device_errors(xnyz_ctx* c) {
+    TRY(fetch_small(c, offsetof(Small, err), sizeof(uint32_t)));
+    return device_errors(c);
 }
 
 QuantParams make_quant(int quantizer, float l2) {
@@ -988,8 +994,8 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
     }
     CUDA_TRY(cudaGetLastError());
     TRY(join_sides(c));
-    TRY(fetch_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8));
-    TRY(check_device_errors(c));
+    TRY(fetch_small(c, offsetof(Small, err), offsetof(Small, codewords) - offsetof(Small, err)));  // err .. totals
+    TRY(device_errors(c));
     const uint64_t gr_bits = c->h_small->totals[0];
     if (!ext && !code_rep.exp_golomb && c->h_small->totals[1] != bits_rep)
         return fail(XNYZ_ERR_CUDA, "Huffman encoder size mismatch (repos)");
@@ -1524,9 +1530,19 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     TRY(join_sides(c));
     hd2.end();
     HostPhase hd3(c, "d3_decode_sync");
-    // count total (for -rle) after the count stream is decoded
-    TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
-    TRY(fetch_small(c, offsetof(Small, fallback), sizeof(uint32_t) * 8));
+    // count total (for -rle) once the count stream is decoded; the fallback flags, totals,
+    // codeword counts and the error word come back in one copy.  A stream whose parallel
+    // decode gave up (rare) is decoded again sequentially and the counts re-summed.
+    auto count_total = [&]() -> xnyz_status {
+        TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
+        if (rle && U) {
+            Prof pr(c, "count_total", 1, 4.0 * U);
+            launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
+        }
+        CUDA_TRY(cudaGetLastError());
+        return fetch_small(c, offsetof(Small, err), offsetof(Small, tile_counters) - offsetof(Small, err));
+    };
+    TRY(count_total());
     bool refetch = false;
     for (auto& j : jobs) {
         if (j.fill || j.fixed_len) continue;
@@ -1536,14 +1552,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
             refetch = true;
         }
     }
-    (void)refetch;
-    if (rle && U) {
-        Prof pr(c, "count_total", 1, 4.0 * U);
-        launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
-    }
-    CUDA_TRY(cudaGetLastError());
-    TRY(fetch_small(c, offsetof(Small, totals), offsetof(Small, tile_counters) - offsetof(Small, totals)));
-    TRY(check_device_errors(c));
+    if (refetch) TRY(count_total());
+    TRY(device_errors(c));
     for (auto& j : jobs)
         if (!j.fill && !j.fixed_len && c->h_small->codewords[j.slot] < j.nsym)
             return fail(XNYZ_ERR_BAD_STREAM, "stream " + std::to_string(j.slot) + " holds " +
@@ -2049,10 +2059,24 @@ xnyz_status xnyz_decompress_device(xnyz_ctx* c, const uint8_t* dev_container, ui
     }
     Header h;
     HostPhase hph(c, "d0_header_device");
+    // The header's fields are read through a 64 KB window of the container copied to the host
+    // at once: a small container's whole header costs one copy, a large one a copy per stream
+    // (each stream's lengths and meta follow the previous stream's data), instead of a copy
+    // and a synchronisation per field.
+    std::vector<uint8_t> win;
+    uint64_t win_off = 0;
     xnyz_status s = parse_header(
         [&](uint64_t off, uint64_t bytes, void* dst) {
-            return cudaMemcpyAsync(dst, d_cont + off, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
-                   cudaStreamSynchronize(st) == cudaSuccess;
+            if (win.empty() || off < win_off || off + bytes > win_off + win.size()) {
+                const uint64_t want = std::min<uint64_t>(len - off, std::max<uint64_t>(bytes, 64u << 10));
+                win.resize(want);
+                win_off = off;
+                if (cudaMemcpyAsync(win.data(), d_cont + off, want, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess)
+                    return false;
+            }
+            std::memcpy(dst, win.data() + (off - win_off), bytes);
+            return true;
         },
         len, rle != 0, h);
     if (s != XNYZ_OK) return s;

@@ -26,6 +26,7 @@ constexpr u32 kFullMask = 0xffffffffu;
 constexpr u32 kErrTimeout = 1u;      // a bounded wait gave up
 constexpr u32 kErrBadStream = 2u;    // a decoder ran past its input or found an invalid code
 constexpr u32 kErrOverflow = 4u;     // an output bound was exceeded
+constexpr u32 kErrPlacement = 8u;    // a scatter computed a position outside its array (skipped)
 
 // Spin limit for look-back waits: ~1 s with the back-off below, then the waiting thread
 // records kErrTimeout and proceeds with what it has (the host reports XNYZ_ERR_TIMEOUT).
