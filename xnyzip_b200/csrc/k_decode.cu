@@ -261,20 +261,31 @@ struct RecoverArgs {
     u32* err;
 };
 
+// Quad index step of a packed quad symbol (see recover_units_kernel): q - 1 modulo 8, 0 for
+// the patch symbol 0.
+__device__ __forceinline__ u32 quad_step(u32 sq) { return (sq & 8u) ? 0u : ((sq + 7u) & 7u); }
+
 // Warp w owns units [512 w, 512 w + 512) of the tile and takes them 32 at a time, one per
 // lane: staged symbols are read without bank conflicts, patches, counts and block starts
 // are read coalesced, and the points of a round are written to consecutive addresses.
-// Pass 1 folds each warp's zero symbols, counts and quad / block segments, pass 2 its
-// repos segments (or SFC sums); the block combines the warps, chained scans combine the
-// tiles, and the final pass rebuilds every running value with warp scans from its warp's
-// starting carry.
+// Phase 1 counts each warp's zero symbols in shared memory (the tile's first patch index
+// then comes from a chained scan that every tile publishes right after staging); phase 2
+// reads the patches and counts once, keeps each unit's repos value (or SFC delta) and count
+// in shared memory, and folds the warp's counts, quad / block / repos segments (or SFC
+// sums); the block combines the warps, one round of chained scans combines the tiles, and
+// the final pass rebuilds every running value with warp scans from its warp's starting
+// carry.  A tile holding a value of 2^32 or more or a count of 2^16 or more (never in a
+// stream the encoder wrote from a cloud's blocks) re-reads them in the final pass instead.
 template <bool DIRECT>
 __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) {
     constexpr int kWarps = kThreads / 32;
     __shared__ u8 srep[kTile];
+    // block mode: quad symbol q's low 3 bits | 8 (q == 0) | 16 (q == 1) | 32 (block start);
+    // the quad index is only used modulo 8, so its running sums need nothing more
     __shared__ u8 squad[DIRECT ? 1 : kTile];
-    __shared__ u8 sstart[DIRECT ? 1 : kTile];
-    __shared__ u32 slot;
+    __shared__ u32 sval[kTile];
+    __shared__ u16 scnt[kTile];
+    __shared__ u32 slot, wide;
     __shared__ u64 wz[kWarps + 1], wc[kWarps + 1], wd[kWarps + 1];
     __shared__ Seg wq[kWarps + 1], wb[kWarps + 1], wr[kWarps + 1];
     __shared__ u64 base_zero, base_count, base_sfc;
@@ -291,13 +302,15 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     const u32 lt = lanemask_lt();
     const bool has_val = a.rep_val != nullptr;
     for (int i = tid; i < 256; i += kThreads) htab[i] = a.hinv ? a.hinv[i] : 0;
+    if (tid == 0) wide = 0;
     for (int i = 0; i < kItems; ++i) {
         const u32 e = (u32)i * kThreads + tid;
         if (e < cnt) {
             srep[e] = has_val ? (u8)1 : a.rep_sym[base + e];
             if (!DIRECT) {
-                squad[e] = a.quad_sym[base + e];
-                sstart[e] = a.is_start[base + e];
+                const u32 qs = a.quad_sym[base + e];
+                squad[e] = (u8)((qs & 7u) | (qs == 0 ? 8u : 0u) | (qs == 1 ? 16u : 0u) |
+                                (a.is_start[base + e] ? 32u : 0u));
             }
         }
     }
@@ -321,50 +334,97 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         return 0;
     };
 
-    // ---- pass 1: zero symbols, counts, quad and block segments per warp ----
+    // ---- phase 1: zero symbols per warp, chained into the tile's first patch index ----
+    if (!has_val) {
+        u64 z = 0;
+        for (int r = 0; r < kItems; ++r) {
+            const u32 e = wfirst + (u32)r * 32u + lane;
+            z += __popc(__ballot_sync(kFullMask, e < cnt && srep[e] == 0));
+        }
+        if (lane == 0) wz[w] = z;
+        __syncthreads();
+        if (tid == 0) warps_exclusive<kThreads / 32>(wz, 0ull, AddOp{});
+        __syncthreads();
+        if (w == 0) {
+            LookBack64 l{a.flag, a.agg, a.inc};
+            const u64 r = warp_lookback_add(l, tile, wz[kWarps], a.err);
+            if (tid == 0) base_zero = r;
+        }
+    } else if (tid < kWarps) {
+        wz[tid] = 0;
+        if (tid == 0) base_zero = 0;
+    }
+    __syncthreads();
+
+    // ---- phase 2: values and counts kept; counts, quad, block, repos segments per warp ----
     {
-        u64 z = 0, c = 0, bc = 0;
+        u64 zc = base_zero + wz[w];
+        u64 c = 0, d = 0, bc = 0, rc = 0;
         u32 qc = 0;
-        bool any_head = false;
+        bool any_head = false, any_rhead = false, big = false;
         for (int r = 0; r < kItems; ++r) {
             const u32 e = wfirst + (u32)r * 32u + lane;
             const bool valid = e < cnt;
-            z += __popc(__ballot_sync(kFullMask, valid && !has_val && srep[e] == 0));
-            if (rle && valid) c += (u64)max(a.counts[base + e], 0);
-            if (!DIRECT) {
-                const bool st = valid && sstart[e] != 0;
+            const u64 v = rep_value(e, valid, zc);
+            const u64 k = rle && valid ? (u64)max(a.counts[base + e], 0) : 0ull;
+            c += k;
+            if (valid) {
+                sval[e] = (u32)v;
+                scnt[e] = (u16)k;
+                big |= (v >> 32) != 0 || (k >> 16) != 0;
+            }
+            if (DIRECT) {
+                d += v;
+            } else {
+                const u32 sq = valid ? squad[e] : 16u;
+                const bool st = (sq & 32u) != 0;
                 const u32 hm = __ballot_sync(kFullMask, st);
-                const u32 qd = valid ? squad[e] : 1u;
-                qc = __shfl_sync(kFullMask, warp_seg_incl<u32>(hm, qd ? qd - 1u : 0u, qc), 31);
+                qc = __shfl_sync(kFullMask, warp_seg_incl<u32>(hm, quad_step(sq), qc), 31);
                 const u32 bv = st ? a.start_block[base + e] : 0u;
                 const u32 last = __shfl_sync(kFullMask, bv, hm ? 31 - __clz(hm) : 0);
                 if (hm) bc = last;
                 any_head |= hm != 0;
+                const u32 hr = __ballot_sync(kFullMask, valid && (st || (sq & 16u) == 0));
+                rc = __shfl_sync(kFullMask, warp_seg_incl<u64>(hr, v, rc), 31);
+                any_rhead |= hr != 0;
             }
         }
         c = warp_sum(c);
+        if (DIRECT) d = warp_sum(d);
+        if (__any_sync(kFullMask, big) && lane == 0) wide = 1;
         if (lane == 0) {
-            wz[w] = z;
             wc[w] = c;
+            wd[w] = d;
             wq[w] = Seg{any_head ? 1ull : 0ull, (u64)qc};
             wb[w] = Seg{any_head ? 1ull : 0ull, bc};
+            wr[w] = Seg{any_rhead ? 1ull : 0ull, rc};
         }
     }
     __syncthreads();
     if (tid == 0) {
-        warps_exclusive<kThreads / 32>(wz, 0ull, AddOp{});
         warps_exclusive<kThreads / 32>(wc, 0ull, AddOp{});
-        if (!DIRECT) {
+        if (DIRECT) {
+            warps_exclusive<kThreads / 32>(wd, 0ull, AddOp{});
+        } else {
             warps_exclusive<kThreads / 32>(wq, Seg{0, 0}, op);
             warps_exclusive<kThreads / 32>(wb, Seg{0, 0}, op);
+            warps_exclusive<kThreads / 32>(wr, Seg{0, 0}, op);
         }
     }
     __syncthreads();
     // one warp per chained scan
     if (w == 0) {
-        LookBack64 l{a.flag, a.agg, a.inc};
-        const u64 r = warp_lookback_add(l, tile, wz[kWarps], a.err);
-        if (tid == 0) base_zero = r;
+        if (DIRECT) {
+            LookBack64 l{a.flag + 4 * ntiles, a.agg + 8ull * ntiles, a.inc + 8ull * ntiles};
+            const u64 r = warp_lookback_add(l, tile, wd[kWarps], a.err);
+            if (tid == 0) base_sfc = r;
+        } else {
+            Seg* ag = reinterpret_cast<Seg*>(a.agg + 8ull * ntiles);
+            Seg* in = reinterpret_cast<Seg*>(a.inc + 8ull * ntiles);
+            const Seg r = warp_lookback(a.flag + 4 * ntiles, ag, in, tile, wr[kWarps], Seg{0, 0}, SegOp{}, LoadSeg{},
+                                        StoreSeg{}, a.err);
+            if (tid == 0) base_rep = r;
+        }
     } else if (w == 1 && rle) {
         LookBack64 l{a.flag + ntiles, a.agg + 2ull * ntiles, a.inc + 2ull * ntiles};
         const u64 r = warp_lookback_add(l, tile, wc[kWarps], a.err);
@@ -385,52 +445,9 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     if (!rle && tid == 0) base_count = 0;
     __syncthreads();
 
-    // ---- pass 2: repos segments (block mode) or SFC sums (direct mode) per warp ----
-    {
-        u64 zc = base_zero + wz[w];
-        u64 d = 0, rc = 0;
-        bool any_head = false;
-        for (int r = 0; r < kItems; ++r) {
-            const u32 e = wfirst + (u32)r * 32u + lane;
-            const bool valid = e < cnt;
-            const u64 v = rep_value(e, valid, zc);
-            if (DIRECT) {
-                d += v;
-            } else {
-                const u32 hm = __ballot_sync(kFullMask, valid && (sstart[e] != 0 || squad[e] != 1));
-                rc = __shfl_sync(kFullMask, warp_seg_incl<u64>(hm, v, rc), 31);
-                any_head |= hm != 0;
-            }
-        }
-        if (DIRECT) d = warp_sum(d);
-        if (lane == 0) {
-            wd[w] = d;
-            wr[w] = Seg{any_head ? 1ull : 0ull, rc};
-        }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (DIRECT) warps_exclusive<kThreads / 32>(wd, 0ull, AddOp{});
-        else warps_exclusive<kThreads / 32>(wr, Seg{0, 0}, op);
-    }
-    __syncthreads();
-    if (w == 0) {
-        if (DIRECT) {
-            LookBack64 l{a.flag + 4 * ntiles, a.agg + 8ull * ntiles, a.inc + 8ull * ntiles};
-            const u64 r = warp_lookback_add(l, tile, wd[kWarps], a.err);
-            if (tid == 0) base_sfc = r;
-        } else {
-            Seg* ag = reinterpret_cast<Seg*>(a.agg + 8ull * ntiles);
-            Seg* in = reinterpret_cast<Seg*>(a.inc + 8ull * ntiles);
-            const Seg r = warp_lookback(a.flag + 4 * ntiles, ag, in, tile, wr[kWarps], Seg{0, 0}, SegOp{}, LoadSeg{},
-                                        StoreSeg{}, a.err);
-            if (tid == 0) base_rep = r;
-        }
-    }
-    __syncthreads();
-
     // ---- final: coordinates, recover, unshift, expand ----
     const QuantParams q = a.rp.q;
+    const bool kept = wide == 0;  // block-uniform
     u64 zc = base_zero + wz[w];
     u64 oc = base_count + wc[w];  // -rle: output position of the warp's first point
     u64 scar = DIRECT ? base_sfc + wd[w] : 0ull;
@@ -440,7 +457,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
     for (int r = 0; r < kItems; ++r) {
         const u32 e = wfirst + (u32)r * 32u + lane;
         const bool valid = e < cnt;
-        const u64 rv = rep_value(e, valid, zc);
+        const u64 rv = kept ? (valid ? (u64)sval[e] : 0ull) : rep_value(e, valid, zc);
         i32 cx = 0, cy = 0, cz = 0;
         if (DIRECT) {
             const u64 sfc = scar + warp_incl_add(rv);
@@ -450,21 +467,21 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
             cy = (i32)gather3(m >> 1);
             cz = (i32)gather3(m >> 2);
         } else {
-            const bool st = valid && sstart[e] != 0;
-            const u32 qd = valid ? squad[e] : 1u;
+            const u32 sq = valid ? squad[e] : 16u;
+            const bool st = (sq & 32u) != 0;
             const u32 hm = __ballot_sync(kFullMask, st);
-            const u32 quadj = warp_seg_incl<u32>(hm, qd ? qd - 1u : 0u, qcar);
+            const u32 quadj = warp_seg_incl<u32>(hm, quad_step(sq), qcar);
             qcar = __shfl_sync(kFullMask, quadj, 31);
             const u32 bv = st ? a.start_block[base + e] : 0u;
             const u32 le = hm & (lt | (1u << lane));
             const u32 bsel = __shfl_sync(kFullMask, bv, le ? 31 - __clz(le) : 0);
             const u64 b = le ? (u64)bsel : bcar;
             bcar = __shfl_sync(kFullMask, b, 31);
-            const u32 hr = __ballot_sync(kFullMask, valid && (st || qd != 1u));
+            const u32 hr = __ballot_sync(kFullMask, valid && (st || (sq & 16u) == 0));
             const u64 reposj = warp_seg_incl<u64>(hr, rv, rcar);
             rcar = __shfl_sync(kFullMask, reposj, 31);
             if (valid) {
-                if (qd == 0) atomicOr(a.err, kErrBadStream);  // quad patches never occur
+                if (sq & 8u) atomicOr(a.err, kErrBadStream);  // quad patches never occur
                 const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
                 // (blk % nx) * 128, (blk / nx % ny) * 128, (blk / nx / ny) * 128, u64 arithmetic
                 const u64 q1 = udiv(blk, a.rp.div_nx), q2 = udiv(q1, a.rp.div_ny);
@@ -481,7 +498,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         // -rle: output position from the count prefix; -normal and cells: one per unit.
         u64 c = 1, opos = base + e;
         if (rle) {
-            c = valid ? (u64)max(a.counts[base + e], 0) : 0ull;
+            c = !valid ? 0ull : kept ? (u64)scnt[e] : (u64)max(a.counts[base + e], 0);
             const u64 incl = warp_incl_add(c);
             opos = oc + incl - c;
             oc += __shfl_sync(kFullMask, incl, 31);
