@@ -446,6 +446,53 @@ __device__ __forceinline__ u64 hilbert_apply(const u8* tab, u64 code, int top, u
     return out;
 }
 
+// gather3 of hilbert_apply(tab, code, top, state) for each axis: the output digit of level
+// l is bit l of x, y and z (bits 0, 1, 2 of the digit), so the transformed levels are
+// de-interleaved as they are produced; levels above `top` pass through gather3.
+__device__ __forceinline__ void hilbert_xyz(const u8* tab, u64 code, int top, u32 state, u32& x, u32& y, u32& z) {
+    const u64 above = top >= 20 ? (code & (top >= 21 ? 0ull : ~0ull << 63)) : (code & (~0ull << (3 * (top + 1))));
+    x = y = z = 0;
+    if (above) {
+        x = gather3(above);
+        y = gather3(above >> 1);
+        z = gather3(above >> 2);
+    }
+    for (int l = top; l >= 0; --l) {
+        const u32 e = tab[state * 8 + ((u32)(code >> (3 * l)) & 7u)];
+        x |= (e & 1u) << l;
+        y |= ((e >> 1) & 1u) << l;
+        z |= ((e >> 2) & 1u) << l;
+        state = e >> 3;
+    }
+}
+
+// hilbert_xyz for top = 5 and a code below 2^18 (the 6 levels of one 64^3 quadrant).
+__device__ __forceinline__ void hilbert_xyz6(const u8* tab, u32 code, u32 state, u32& x, u32& y, u32& z) {
+    x = y = z = 0;
+#pragma unroll
+    for (int l = 5; l >= 0; --l) {
+        const u32 e = tab[state * 8 + ((code >> (3 * l)) & 7u)];
+        x |= (e & 1u) << l;
+        y |= ((e >> 1) & 1u) << l;
+        z |= ((e >> 2) & 1u) << l;
+        state = e >> 3;
+    }
+}
+
+// hilbert_apply(tab, morton3(x, y, z), 5, state) for x, y, z below 64: the input digit of
+// level l is bit l of x, y and z, so the interleave is done as the levels are consumed.
+__device__ __forceinline__ u32 hilbert_code6(const u8* tab, u32 x, u32 y, u32 z, u32 state) {
+    u32 out = 0;
+#pragma unroll
+    for (int l = 5; l >= 0; --l) {
+        const u32 d = ((x >> l) & 1u) | (((y >> l) & 1u) << 1) | (((z >> l) & 1u) << 2);
+        const u32 e = tab[state * 8 + d];
+        out |= (e & 7u) << (3 * l);
+        state = e >> 3;
+    }
+    return out;
+}
+
 // ------------------------------------------------------------- bit writers --------------
 // Stream words are 32-bit; the output buffer must be zeroed and 4-byte aligned.
 // MSB-first streams: stream bit p is bit (7 - p%8) of byte p/8; a 32-bit word k then holds

@@ -462,10 +462,17 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         if (DIRECT) {
             const u64 sfc = scar + warp_incl_add(rv);
             scar = __shfl_sync(kFullMask, sfc, 31);
-            const u64 m = a.rp.hilbert ? hilbert_apply(htab, sfc, a.rp.bits, 0u) : sfc;
-            cx = (i32)gather3(m);
-            cy = (i32)gather3(m >> 1);
-            cz = (i32)gather3(m >> 2);
+            u32 gx, gy, gz;
+            if (a.rp.hilbert) {
+                hilbert_xyz(htab, sfc, a.rp.bits, 0u, gx, gy, gz);
+            } else {
+                gx = gather3(sfc);
+                gy = gather3(sfc >> 1);
+                gz = gather3(sfc >> 2);
+            }
+            cx = (i32)gx;
+            cy = (i32)gy;
+            cz = (i32)gz;
         } else {
             const u32 sq = valid ? squad[e] : 16u;
             const bool st = (sq & 32u) != 0;
@@ -486,13 +493,19 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
                 // (blk % nx) * 128, (blk / nx % ny) * 128, (blk / nx / ny) * 128, u64 arithmetic
                 const u64 q1 = udiv(blk, a.rp.div_nx), q2 = udiv(q1, a.rp.div_ny);
                 const u64 pbx = (blk - q1 * a.rp.nx) * 128, pby = (q1 - q2 * a.rp.ny) * 128, pbz = q2 * 128;
-                u64 m = reposj;
-                if (a.rp.hilbert)
-                    m = reposj < (1ull << 18) ? hilbert_apply(htab, reposj, 5, a.rp.hstart_inv)
-                                              : hilbert_apply(htab, reposj, 20, 0u);
-                cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64 + (u64)gather3(m));
-                cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gather3(m >> 1));
-                cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gather3(m >> 2));
+                u32 gx, gy, gz;
+                if (!a.rp.hilbert) {
+                    gx = gather3(reposj);
+                    gy = gather3(reposj >> 1);
+                    gz = gather3(reposj >> 2);
+                } else if (reposj < (1ull << 18)) {
+                    hilbert_xyz6(htab, (u32)reposj, a.rp.hstart_inv, gx, gy, gz);
+                } else {
+                    hilbert_xyz(htab, reposj, 20, 0u, gx, gy, gz);
+                }
+                cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64 + (u64)gx);
+                cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gy);
+                cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gz);
             }
         }
         // -rle: output position from the count prefix; -normal and cells: one per unit.

@@ -186,43 +186,138 @@ __device__ __forceinline__ void head_range(int head, int& lo, int& n) {
     n = head ? kParamOutputsW : kParamOutputsK;
 }
 
-__global__ void __launch_bounds__(THREADS) forward_kernel(const float* __restrict__ prm, const float* __restrict__ feats,
-                                                          u64 count, u8* __restrict__ wout, u8* __restrict__ kout,
-                                                          float* __restrict__ conf, float* __restrict__ logits) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Weights& s = *reinterpret_cast<Weights*>(smem_raw);
-    WarpTile* tiles = reinterpret_cast<WarpTile*>(smem_raw + sizeof(Weights));
-    load_weights(s, prm, false);
-    __syncthreads();
-    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpTile& w = tiles[wi];
-    const u64 ntiles = (count + 15) / 16;
-    for (u64 tile = (u64)blockIdx.x * WARPS + wi; tile < ntiles; tile += (u64)gridDim.x * WARPS) {
-        const u64 s0 = tile * 16;
-        warp_forward(s, w, feats, s0, count);
-        const int r = lane & 15, head = lane >> 4;
-        const u64 row = s0 + r;
-        int lo, nn;
-        head_range(head, lo, nn);
-        float m = -INFINITY;
-        int am = 0;
-        for (int j = 0; j < nn; ++j) {
-            const float v = w.L[r * NO + lo + j];
-            if (v > m) {
+// Inference layout: row pitches of 56 and 72 bf16 (28 and 36 words), so the 8 row groups of
+// an MMA fragment load fall in distinct banks; no backward tiles, so 12 warps of 16 samples
+// fit twice per SM.
+constexpr int LI = NI + 8;
+constexpr int LH = NH + 8;
+constexpr int FWARPS = 12;
+constexpr int FTHREADS = 32 * FWARPS;
+
+struct FwdShared {
+    bf16 W1[NH * LI];  // [out][in]
+    bf16 W2[NH * LH];
+    bf16 W3[NO * LH];
+    float b1[NH], b2[NH], b3[NO];
+    struct Tile {
+        bf16 X[16 * LI];
+        bf16 H1[16 * LH];
+        bf16 H2[16 * LH];
+    } t[FWARPS];
+};
+
+// Argmax (first maximum, 0 when no logit exceeds -inf) and 1 / sum(exp(logit - max)) of
+// one head for row g + 8 * half of the warp's C fragments, combined over the 4 lanes that
+// hold the row.
+template <int NT0, int NT1>
+__device__ __forceinline__ void head_argmax(const float (&acc)[NO / 8][4], const float* b3, int half, int lo, int hi,
+                                            int& am, float& conf) {
+    const int t = threadIdx.x & 3;
+    float m = -INFINITY;
+    int a = 1 << 10;
+#pragma unroll
+    for (int nt = NT0; nt < NT1; ++nt)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int c = nt * 8 + 2 * t + j;
+            const float v = acc[nt][2 * half + j] + b3[c];
+            if (c < hi && v > m) {
                 m = v;
-                am = j;
+                a = c - lo;
             }
         }
-        float se = 0.f;
-        for (int j = 0; j < nn; ++j) se += __expf(w.L[r * NO + lo + j] - m);
-        if (row < count) {
-            if (head == 0) kout[row] = (u8)am;
-            else wout[row] = (u8)am;
-            if (conf) conf[row * 2 + head] = 1.0f / se;
-            if (logits)
-                for (int j = 0; j < nn; ++j) logits[row * (kParamOutputsK + kParamOutputsW) + lo + j] = w.L[r * NO + lo + j];
+#pragma unroll
+    for (int off = 1; off <= 2; off <<= 1) {
+        const float om = __shfl_xor_sync(kFullMask, m, off);
+        const int oa = __shfl_xor_sync(kFullMask, a, off);
+        if (om > m || (om == m && oa < a)) {
+            m = om;
+            a = oa;
+        }
+    }
+    float se = 0.f;
+#pragma unroll
+    for (int nt = NT0; nt < NT1; ++nt)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int c = nt * 8 + 2 * t + j;
+            if (c < hi) se += __expf(acc[nt][2 * half + j] + b3[c] - m);
+        }
+    se += __shfl_xor_sync(kFullMask, se, 1);
+    se += __shfl_xor_sync(kFullMask, se, 2);
+    am = a == (1 << 10) ? 0 : a;
+    conf = 1.0f / se;
+}
+
+__global__ void __launch_bounds__(FTHREADS) forward_kernel(const float* __restrict__ prm, const float* __restrict__ feats,
+                                                           u64 count, u8* __restrict__ wout, u8* __restrict__ kout,
+                                                           float* __restrict__ conf, float* __restrict__ logits) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FwdShared& s = *reinterpret_cast<FwdShared*>(smem_raw);
+    for (int i = threadIdx.x; i < NH * NI; i += FTHREADS)
+        s.W1[(i / NI) * LI + i % NI] = __float2bfloat16_rn(prm[oW1 + i]);
+    for (int i = threadIdx.x; i < NH * NH; i += FTHREADS)
+        s.W2[(i / NH) * LH + i % NH] = __float2bfloat16_rn(prm[oW2 + i]);
+    for (int i = threadIdx.x; i < NO * NH; i += FTHREADS)
+        s.W3[(i / NH) * LH + i % NH] = __float2bfloat16_rn(prm[oW3 + i]);
+    for (int i = threadIdx.x; i < NH; i += FTHREADS) {
+        s.b1[i] = prm[ob1 + i];
+        s.b2[i] = prm[ob2 + i];
+    }
+    for (int i = threadIdx.x; i < NO; i += FTHREADS) s.b3[i] = prm[ob3 + i];
+    __syncthreads();
+    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    FwdShared::Tile& w = s.t[wi];
+    const u64 ntiles = (count + 15) / 16;
+    for (u64 tile = (u64)blockIdx.x * FWARPS + wi; tile < ntiles; tile += (u64)gridDim.x * FWARPS) {
+        const u64 s0 = tile * 16;
+        for (int i = lane; i < 16 * NI; i += 32) {
+            const int r = i / NI, c = i % NI;
+            const u64 row = s0 + r;
+            w.X[r * LI + c] =
+                __float2bfloat16_rn((row < count && c < kParamInputs) ? feats[row * kParamFeatures + c] : 0.f);
         }
         __syncwarp();
+        {
+            float acc[NH / 8][4] = {};
+            warp_gemm<NI / 16, NH / 8>(acc, RowPairs{w.X, LI}, RowPairs{s.W1, LI});
+            store_act<NH / 8>(w.H1, LH, acc, s.b1, true);
+        }
+        __syncwarp();
+        {
+            float acc[NH / 8][4] = {};
+            warp_gemm<NH / 16, NH / 8>(acc, RowPairs{w.H1, LH}, RowPairs{s.W2, LH});
+            store_act<NH / 8>(w.H2, LH, acc, s.b2, true);
+        }
+        __syncwarp();
+        float acc[NO / 8][4] = {};
+        warp_gemm<NH / 16, NO / 8>(acc, RowPairs{w.H2, LH}, RowPairs{s.W3, LH});
+        __syncwarp();  // X, H1, H2 are rewritten by the next tile
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const u64 row = s0 + g + 8 * half;
+            int ak, aw;
+            float ck, cw;
+            head_argmax<0, kParamOutputsK / 8>(acc, s.b3, half, 0, kParamOutputsK, ak, ck);
+            head_argmax<kParamOutputsK / 8, NO / 8>(acc, s.b3, half, kParamOutputsK, kParamOutputsK + kParamOutputsW,
+                                                    aw, cw);
+            if (row < count) {
+                if (t == 0) kout[row] = (u8)ak;
+                if (t == 1) wout[row] = (u8)aw;
+                if (conf && t == 2) conf[row * 2] = ck;
+                if (conf && t == 3) conf[row * 2 + 1] = cw;
+                if (logits) {
+#pragma unroll
+                    for (int nt = 0; nt < NO / 8; ++nt)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j) {
+                            const int c = nt * 8 + 2 * t + j;
+                            if (c < kParamOutputsK + kParamOutputsW)
+                                logits[row * (kParamOutputsK + kParamOutputsW) + c] = acc[nt][2 * half + j] + s.b3[c];
+                        }
+                }
+            }
+        }
     }
 }
 
@@ -387,12 +482,12 @@ size_t mlp_gather_floats(uint64_t count) {
 void launch_mlp_forward(const float* prm, const float* feats, uint64_t count, uint8_t* w, uint8_t* k, float* conf,
                         float* logits, cudaStream_t st) {
     if (!count) return;
-    const int smem = (int)(sizeof(Weights) + WARPS * sizeof(WarpTile));
+    const int smem = (int)sizeof(FwdShared);
     cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const u64 ntiles = (count + 15) / 16;
-    u64 ctas = (ntiles + WARPS - 1) / WARPS;
-    if (ctas > 148 * 4) ctas = 148 * 4;
-    forward_kernel<<<(unsigned)ctas, THREADS, smem, st>>>(prm, feats, count, w, k, conf, logits);
+    u64 ctas = (ntiles + FWARPS - 1) / FWARPS;
+    if (ctas > 148 * 2) ctas = 148 * 2;  // two CTAs per SM (shared memory)
+    forward_kernel<<<(unsigned)ctas, FTHREADS, smem, st>>>(prm, feats, count, w, k, conf, logits);
 }
 
 void launch_mlp_train(const float* prm, const float* feats, const uint8_t* wlab, const uint8_t* klab,

@@ -255,8 +255,7 @@ __device__ __forceinline__ u64 block_key(i32 x, i32 y, i32 z, const BlockKeyPara
     const u64 X = (u64)(i64)x, Y = (u64)(i64)y, Z = (u64)(i64)z;
     const u64 cx = X >> 6, cy = Y >> 6, cz = Z >> 6;
     const u32 dx = (u32)(X & 63u), dy = (u32)(Y & 63u), dz = (u32)(Z & 63u);
-    u64 m = morton3((i32)dx, (i32)dy, (i32)dz);
-    if (kp.hilbert) m = hilbert_apply(htab, m, 5, kp.hstart);
+    const u64 m = kp.hilbert ? (u64)hilbert_code6(htab, dx, dy, dz, kp.hstart) : morton3((i32)dx, (i32)dy, (i32)dz);
     const u64 quad = (cx & 1u) | ((cy & 1u) << 1) | ((cz & 1u) << 2);
     const u64 low = (quad << 18) | m;
     const u64 xy = (cx >> 1) + (cy >> 1) * kp.nx;
