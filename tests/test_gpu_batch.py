@@ -98,3 +98,31 @@ def test_batch_roundtrip_device_and_autotune(xnyz, ctx):
     finally:
         one.close()
         b.close()
+
+
+def test_learned_mode_survives_workspace_growth_and_trim(xnyz):
+    """The predictor's parameters live beside the context's workspace: growing the device
+    container buffer (a larger cloud) or trimming the workspace must leave them in place, so a
+    learned-mode compress after either writes the same container as before."""
+    import torch
+    from xnyzip_b200 import synthetic as S
+    from xnyzip_b200 import verify as V
+    small = torch.from_numpy(S.terrain(20_000, 61, extent=300.0, amplitude=2.0, wavelength=90.0)).cuda()
+    large = torch.from_numpy(S.terrain(900_000, 62, extent=900.0, amplitude=2.0, wavelength=90.0)).cuda()
+    c = xnyz.Context(0)
+    try:
+        c.set_block_mode(2)
+
+        def digest(x):
+            p, ln = c.compress_device(x.data_ptr(), x.shape[0], 1, 0.01, True, True)
+            torch.cuda.synchronize()
+            return ln, V.sha256(V.device_view(p, (ln,), "|u1", x.device))
+
+        first = digest(small)
+        digest(large)  # grows the device container buffer
+        assert digest(small) == first
+        from xnyzip_b200 import _native as N
+        N.check(N.trim(c.handle))
+        assert digest(small) == first
+    finally:
+        c.close()

@@ -1735,7 +1735,6 @@ xnyz_status xnyz_trim(xnyz_ctx* c) {
     if (c->arena.base) cudaFree(c->arena.base);
     c->arena = Arena{};
     if (c->d_container) cudaFree(c->d_container);
-    if (c->d_model) cudaFree(c->d_model);
     c->d_container = nullptr;
     c->d_container_cap = 0;
     return XNYZ_OK;
@@ -1900,7 +1899,6 @@ xnyz_status xnyz_compress_device(xnyz_ctx* c, const float* xyz, uint64_t n, cons
     if (c->d_container_cap < clen + 64) {
         CUDA_TRY(cudaStreamSynchronize(st));
         if (c->d_container) cudaFree(c->d_container);
-    if (c->d_model) cudaFree(c->d_model);
         c->d_container = nullptr;
         const size_t want = align_up(clen + clen / 4 + 64, 1 << 20);
         CUDA_TRY(cudaMalloc(&c->d_container, want));

@@ -9,10 +9,12 @@
 // Per pass: each warp ranks its 512 keys against warp-private digit counters, finding the
 // lanes that share a digit through a per-warp bit mask in shared memory (one atomicOr per
 // lane: cheaper than match.any, which serialises on the address-divergence pipe), the
-// block turns warp counts into tile-local digit offsets, one thread per
-// digit resolves the tile's global base by look-back over the previous tiles' digit counts
-// (epoch-tagged 64-bit status words, so the status array is never cleared between passes),
-// keys are staged in shared memory in digit order and written out in coalesced runs.
+// block turns warp counts into tile-local digit offsets, one thread per digit publishes the
+// tile's count and starts the look-back over the previous tiles' digit counts (two
+// predecessors per step; epoch-tagged 64-bit status words, so the status array is never
+// cleared between passes), the keys are staged in shared memory in digit order while those
+// loads are in flight, and, once the look-back has resolved the tile's global bases, written
+// out in coalesced runs.
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -33,29 +35,44 @@ __device__ __forceinline__ u64 pack_status(u32 epoch, u32 flag, u64 count) {
     return ((u64)epoch << 50) | ((u64)flag << 48) | (count & ((1ull << 48) - 1));
 }
 
-__device__ u64 digit_lookback(u64* status, u32 tile, u32 d, u64 count, u32 epoch, u32* err) {
-    if (tile == 0) {
-        st_volatile(&status[d], pack_status(epoch, 2, count));
-        return 0;
-    }
-    st_volatile(&status[(u64)tile * kRadix + d], pack_status(epoch, 1, count));
+// Look-back of digit d over the previous tiles' status words, kLookWindow predecessors per
+// step (their loads in flight together).  `pre` holds the first window, loaded by the caller
+// before it stages the tile's keys, so that the wait overlaps that work.  Publishes the
+// tile's inclusive count and returns the count of digit d in all previous tiles.
+constexpr int kLookWindow = 2;
+
+__device__ u64 digit_lookback(u64* status, u32 tile, u32 d, u64 count, u32 epoch, u32* err, const u64* pre0) {
     u64 acc = 0;
     long long t = (long long)tile - 1;
+    u64 pre[kLookWindow];
+#pragma unroll
+    for (int q = 0; q < kLookWindow; ++q) pre[q] = pre0[q];
     u32 spins = 0;
     while (t >= 0) {
-        const u64 s = ld_volatile(&status[(u64)t * kRadix + d]);
-        const u32 e = (u32)(s >> 50), f = (u32)(s >> 48) & 3u;
-        if (e != epoch || f == 0) {
+        int used = 0;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < kLookWindow; ++q) {
+            if (done || t - q < 0) break;
+            const u64 s = pre[q];
+            const u32 e = (u32)(s >> 50), f = (u32)(s >> 48) & 3u;
+            if (e != epoch || f == 0) break;  // not published yet: re-read from here
+            acc += s & ((1ull << 48) - 1);
+            ++used;
+            if (f == 2) done = true;
+        }
+        if (done) break;
+        if (used == 0) {
             if (++spins > kSpinLimit) {
                 atomicOr(err, kErrTimeout);
                 break;
             }
-            if (spins > 64) __nanosleep(64);
-            continue;
+            if (spins > 8) __nanosleep(32);
         }
-        acc += s & ((1ull << 48) - 1);
-        if (f == 2) break;
-        --t;
+        t -= used;
+#pragma unroll
+        for (int q = 0; q < kLookWindow; ++q)
+            pre[q] = t - q >= 0 ? ld_volatile(&status[(u64)(t - q) * kRadix + d]) : 0ull;
     }
     st_volatile(&status[(u64)tile * kRadix + d], pack_status(epoch, 2, acc + count));
     return acc;
@@ -136,8 +153,17 @@ __global__ void __launch_bounds__(kThreads, PAYLOAD ? 3 : 4) sort_pass_kernel(co
     u32 total;
     const u32 start = block_exclusive<kThreads>(tile_count, 0u, AddOp{}, scratch, total);
     dstart[tid] = start;
-    const u64 before = digit_lookback(status, tile, (u32)tid, tile_count, epoch, err);
-    gbase[tid] = (u64)offsets[tid] + before;
+    // Digit tid: publish the tile's count and load the first look-back window; the keys are
+    // staged while those loads are in flight, then the look-back completes.
+    u64 pre[kLookWindow];
+    if (tile == 0) {
+        st_volatile(&status[tid], pack_status(epoch, 2, tile_count));
+    } else {
+        st_volatile(&status[(u64)tile * kRadix + tid], pack_status(epoch, 1, tile_count));
+#pragma unroll
+        for (int q = 0; q < kLookWindow; ++q)
+            pre[q] = (long long)tile - 1 - q >= 0 ? ld_volatile(&status[(u64)(tile - 1 - q) * kRadix + tid]) : 0ull;
+    }
     __syncthreads();
 
 #pragma unroll
@@ -149,6 +175,8 @@ __global__ void __launch_bounds__(kThreads, PAYLOAD ? 3 : 4) sort_pass_kernel(co
             if (PAYLOAD) svals[p] = v[i];
         }
     }
+    const u64 before = tile == 0 ? 0ull : digit_lookback(status, tile, (u32)tid, tile_count, epoch, err, pre);
+    gbase[tid] = (u64)offsets[tid] + before;
     __syncthreads();
 
     const u32 cnt = (u32)min((u64)kTile, n - base);
