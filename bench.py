@@ -68,11 +68,11 @@ def vname(v):
     return f"{QNAME[q]}_{l2}" + ("" if (hil, rle) == (1, 1) else f"_{'h' if hil else 'z'}_{'rle' if rle else 'normal'}")
 QNAME = {0: "cube", 1: "to"}
 # DRAM bytes (read + write) per key of one keys-only sort pass, from an ncu capture of one
-# sort_pass_kernel<0> launch over 32M terrain keys (263.6 MB read + 222.8 MB written): below
+# sort_pass_kernel<0> launch over 24M terrain keys (199.4 MB read + 154.5 MB written): below
 # the 16 algorithmic bytes because part of the input is still in L2 from the previous pass.
 # Scaled by the keys of a launch; the L2 share shrinks as the cloud grows, so at 64M keys
 # this is a lower bound on the traffic.
-SORT_PASS_DRAM_BYTES_PER_KEY = (263.600384e6 + 222.781184e6) / 32e6
+SORT_PASS_DRAM_BYTES_PER_KEY = (199.396608e6 + 154.480640e6) / 24e6
 METRIC = "compress+decompress GB/s (12 B/point input) at fixed L2 bound"
 
 
@@ -475,7 +475,7 @@ def run_gpu(args):
                          "traffic": (round(SORT_PASS_DRAM_BYTES_PER_KEY * per_launch_bytes / 16.0)
                                      if dom_name == "sort_pass" and per_launch_bytes and args.workload == "terrain"
                                      else None),
-                         "traffic_source": "ncu DRAM bytes per key of a keys-only pass over 32M keys, "
+                         "traffic_source": "ncu DRAM bytes per key of a keys-only pass over 24M keys, "
                                            "scaled to this launch's keys",
                          "bytes_per_launch": per_launch_bytes, "ms_per_launch": round(per_launch_ms, 4),
                          "pipeline_achieved": round(stage_bytes / (stage_ms / 1e3) / 1e9, 1),
