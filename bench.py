@@ -1030,7 +1030,7 @@ def main():
     ap.add_argument("--e2e-mode", default="roundtrip", choices=["roundtrip", "phases"],
                     help="e2e: xnyz_batch_roundtrip (each chunk compressed and decompressed on one worker) or "
                          "xnyz_batch_compress then xnyz_batch_decompress")
-    ap.add_argument("--pipes", type=int, default=3, help="contexts (streams) the timed step spreads the variants over")
+    ap.add_argument("--pipes", type=int, default=6, help="contexts (streams) the timed step spreads the variants over")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-points", type=int, default=1_000_000)
     ap.add_argument("--chunk", type=int, default=150_000, help="points per chunk (e2e and the reference arm)")

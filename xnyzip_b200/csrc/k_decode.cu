@@ -277,7 +277,7 @@ __device__ __forceinline__ u32 quad_step(u32 sq) { return (sq & 8u) ? 0u : ((sq 
 // carry.  A tile holding a value of 2^32 or more or a count of 2^16 or more (never in a
 // stream the encoder wrote from a cloud's blocks) re-reads them in the final pass instead.
 template <bool DIRECT>
-__global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) {
+__global__ void __launch_bounds__(kThreads, 6) recover_units_kernel(RecoverArgs a) {
     constexpr int kWarps = kThreads / 32;
     __shared__ u8 srep[kTile];
     // block mode: quad symbol q's low 3 bits | 8 (q == 0) | 16 (q == 1) | 32 (block start);
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         u64 zc = base_zero + wz[w];
         u64 c = 0, d = 0, bc = 0, rc = 0;
         u32 qc = 0;
-        bool any_head = false, any_rhead = false, big = false;
+        bool any_head = false, any_rhead = false, big = false, w26 = false;
         for (int r = 0; r < kItems; ++r) {
             const u32 e = wfirst + (u32)r * 32u + lane;
             const bool valid = e < cnt;
@@ -372,6 +372,7 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
                 sval[e] = (u32)v;
                 scnt[e] = (u16)k;
                 big |= (v >> 32) != 0 || (k >> 16) != 0;
+                w26 |= (v >> 26) != 0;
             }
             if (DIRECT) {
                 d += v;
@@ -391,7 +392,8 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
         }
         c = warp_sum(c);
         if (DIRECT) d = warp_sum(d);
-        if (__any_sync(kFullMask, big) && lane == 0) wide = 1;
+        const bool anybig = __any_sync(kFullMask, big), any26 = __any_sync(kFullMask, w26);
+        if (lane == 0 && (anybig || any26)) atomicOr(&wide, (anybig ? 1u : 0u) | (any26 ? 2u : 0u));
         if (lane == 0) {
             wc[w] = c;
             wd[w] = d;
@@ -447,20 +449,34 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
 
     // ---- final: coordinates, recover, unshift, expand ----
     const QuantParams q = a.rp.q;
-    const bool kept = wide == 0;  // block-uniform
+    // block-uniform: values and counts kept in shared memory; and, with every value below 2^26
+    // and every count below 2^16, the round's prefix sums fit 32 bits
+    const bool kept = (wide & 1u) == 0;
+    const bool narrow = wide == 0;
     u64 zc = base_zero + wz[w];
     u64 oc = base_count + wc[w];  // -rle: output position of the warp's first point
     u64 scar = DIRECT ? base_sfc + wd[w] : 0ull;
     u32 qcar = DIRECT ? 0u : (u32)op(base_quad, wq[w]).sum;
-    u64 bcar = DIRECT ? 0ull : op(base_blk, wb[w]).sum;
     u64 rcar = DIRECT ? 0ull : op(base_rep, wr[w]).sum;
+    // corner of the block of the warp's current unit ((blk % nx) * 128, (blk / nx % ny) * 128,
+    // (blk / nx / ny) * 128 in u64 arithmetic, kept modulo 2^32 like the cell coordinates they
+    // are added to): computed where a block starts, carried to the units after it
+    u32 pcx = 0, pcy = 0, pcz = 0;
+    auto corner = [&](u64 b, u32& x, u32& y, u32& z) {
+        const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
+        const u64 q1 = udiv(blk, a.rp.div_nx), q2 = udiv(q1, a.rp.div_ny);
+        x = (u32)((blk - q1 * a.rp.nx) * 128);
+        y = (u32)((q1 - q2 * a.rp.ny) * 128);
+        z = (u32)(q2 * 128);
+    };
+    if (!DIRECT) corner(op(base_blk, wb[w]).sum, pcx, pcy, pcz);
     for (int r = 0; r < kItems; ++r) {
         const u32 e = wfirst + (u32)r * 32u + lane;
         const bool valid = e < cnt;
         const u64 rv = kept ? (valid ? (u64)sval[e] : 0ull) : rep_value(e, valid, zc);
         i32 cx = 0, cy = 0, cz = 0;
         if (DIRECT) {
-            const u64 sfc = scar + warp_incl_add(rv);
+            const u64 sfc = scar + (narrow ? (u64)warp_incl_add((u32)rv) : warp_incl_add(rv));
             scar = __shfl_sync(kFullMask, sfc, 31);
             u32 gx, gy, gz;
             if (a.rp.hilbert) {
@@ -479,20 +495,30 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
             const u32 hm = __ballot_sync(kFullMask, st);
             const u32 quadj = warp_seg_incl<u32>(hm, quad_step(sq), qcar);
             qcar = __shfl_sync(kFullMask, quadj, 31);
-            const u32 bv = st ? a.start_block[base + e] : 0u;
+            u32 sx = 0, sy = 0, sz = 0;
+            if (st) corner(a.start_block[base + e], sx, sy, sz);
             const u32 le = hm & (lt | (1u << lane));
-            const u32 bsel = __shfl_sync(kFullMask, bv, le ? 31 - __clz(le) : 0);
-            const u64 b = le ? (u64)bsel : bcar;
-            bcar = __shfl_sync(kFullMask, b, 31);
+            const int src = le ? 31 - __clz(le) : 0;
+            sx = __shfl_sync(kFullMask, sx, src);
+            sy = __shfl_sync(kFullMask, sy, src);
+            sz = __shfl_sync(kFullMask, sz, src);
+            const u32 pbx = le ? sx : pcx, pby = le ? sy : pcy, pbz = le ? sz : pcz;
+            pcx = __shfl_sync(kFullMask, pbx, 31);
+            pcy = __shfl_sync(kFullMask, pby, 31);
+            pcz = __shfl_sync(kFullMask, pbz, 31);
             const u32 hr = __ballot_sync(kFullMask, valid && (st || (sq & 16u) == 0));
-            const u64 reposj = warp_seg_incl<u64>(hr, rv, rcar);
+            u64 reposj;
+            if (narrow) {
+                const u32 v32 = (u32)rv, inc = warp_incl_add(v32);
+                const u32 lr = hr & (lt | (1u << lane));
+                const u32 before = __shfl_sync(kFullMask, inc - v32, lr ? 31 - __clz(lr) : 0);
+                reposj = lr ? (u64)(inc - before) : rcar + (u64)inc;
+            } else {
+                reposj = warp_seg_incl<u64>(hr, rv, rcar);
+            }
             rcar = __shfl_sync(kFullMask, reposj, 31);
             if (valid) {
                 if (sq & 8u) atomicOr(a.err, kErrBadStream);  // quad patches never occur
-                const u64 blk = b < a.nblocks ? a.blk_ids[b] : 0ull;
-                // (blk % nx) * 128, (blk / nx % ny) * 128, (blk / nx / ny) * 128, u64 arithmetic
-                const u64 q1 = udiv(blk, a.rp.div_nx), q2 = udiv(q1, a.rp.div_ny);
-                const u64 pbx = (blk - q1 * a.rp.nx) * 128, pby = (q1 - q2 * a.rp.ny) * 128, pbz = q2 * 128;
                 u32 gx, gy, gz;
                 if (!a.rp.hilbert) {
                     gx = gather3(reposj);
@@ -503,16 +529,16 @@ __global__ void __launch_bounds__(kThreads) recover_units_kernel(RecoverArgs a) 
                 } else {
                     hilbert_xyz(htab, reposj, 20, 0u, gx, gy, gz);
                 }
-                cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64 + (u64)gx);
-                cy = (i32)(pby + ((quadj & 2u) >> 1) * 64 + (u64)gy);
-                cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64 + (u64)gz);
+                cx = (i32)(pbx + ((quadj & 1u) >> 0) * 64u + gx);
+                cy = (i32)(pby + ((quadj & 2u) >> 1) * 64u + gy);
+                cz = (i32)(pbz + ((quadj & 4u) >> 2) * 64u + gz);
             }
         }
         // -rle: output position from the count prefix; -normal and cells: one per unit.
         u64 c = 1, opos = base + e;
         if (rle) {
             c = !valid ? 0ull : kept ? (u64)scnt[e] : (u64)max(a.counts[base + e], 0);
-            const u64 incl = warp_incl_add(c);
+            const u64 incl = narrow ? (u64)warp_incl_add((u32)c) : warp_incl_add(c);
             opos = oc + incl - c;
             oc += __shfl_sync(kFullMask, incl, 31);
         }

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     __shared__ u32 slot;
     __shared__ u64 sbase[3];
     __shared__ u32 hrep[256], frep[256], hquad[16], fquad[16];
-    __shared__ u32 mrep[kThreads / 32][256], mquad[kThreads / 32][16];
+    __shared__ u32 mrep[kThreads / 32][256];
     __shared__ u64 psum[kThreads / 32];
 
     const u32 tile = claim_tile(tile_counter, &slot);
@@ -95,7 +95,6 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
         fquad[tid] = 0xffffffffu;
     }
     for (int i = tid; i < (kThreads / 32) * 256; i += kThreads) (&mrep[0][0])[i] = 0u;
-    if (tid < (kThreads / 32) * 16) (&mquad[0][0])[tid] = 0u;
     __syncthreads();
 
     // Element e of the tile: flags (bit0 head, bit1 patch, bit2 new block, bits 8..15 quad
@@ -179,6 +178,9 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
     u64 bb = sbase[2] + ((wex >> 42) & ((1ull << 21) - 1));
     const u32 lt = lanemask_lt();
     u64 mysum = 0;
+    // quad symbols are 1..8 (qd = 0..7): lane v < 8 counts symbol v + 1 from three ballots of
+    // its bits, and keeps the unit of its first occurrence
+    u32 qn = 0, qf = 0xffffffffu;
     for (int r = 0; r < kItems; ++r) {
         const u32 e = wfirst + (u32)r * 32u + lane;
         u64 vi, idi;
@@ -207,10 +209,23 @@ __global__ void __launch_bounds__(kThreads) units_kernel(const u64* __restrict__
             if (rle) out.unit_pos[u] = (u32)(base + e);
         }
         hist_add_masked(mrep[w], hrep, frep, head, sym, (u32)u);
-        if (!DIRECT) hist_add_masked(mquad[w], hquad, fquad, head, qsym, (u32)u);
+        if (!DIRECT) {
+            const u32 qb = qsym - 1u;
+            const u32 b0 = __ballot_sync(kFullMask, head && (qb & 1u)), b1 = __ballot_sync(kFullMask, head && (qb & 2u)),
+                      b2 = __ballot_sync(kFullMask, head && (qb & 4u));
+            const u32 mv = hm & ((lane & 1u) ? b0 : ~b0) & ((lane & 2u) ? b1 : ~b1) & ((lane & 4u) ? b2 : ~b2);
+            if (lane < 8u && mv) {
+                qn += (u32)__popc(mv);
+                if (qf == 0xffffffffu) qf = (u32)(uu + (u32)__popc(hm & ((1u << (__ffs(mv) - 1)) - 1u)));
+            }
+        }
         uu += __popc(hm);
         pp += __popc(pm);
         bb += __popc(bm);
+    }
+    if (!DIRECT && lane < 8u && qn) {
+        atomicAdd(&hquad[lane + 1], qn);
+        atomicMin(&fquad[lane + 1], qf);
     }
     for (int d = 16; d > 0; d >>= 1) mysum += __shfl_xor_sync(kFullMask, mysum, d);
     if (lane_id() == 0) psum[tid >> 5] = mysum;
