@@ -139,9 +139,9 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
 
     // Running values along the warp's blocks: blk (block id), cnt (block count = inclusive
     // sum of the count deltas), start (first unit of the block = exclusive sum of the
-    // counts).  One pass from zero gives the warp's aggregates, the second from the true
-    // carries writes the outputs.
-    auto pass = [&](u64& blk, u64& cnt, u64& start, bool write) {
+    // counts).  The warp's aggregates need no scans (below); the pass from the true carries
+    // writes the outputs.
+    auto pass = [&](u64& blk, u64& cnt, u64& start) {
         for (int r = 0; r < kItems; ++r) {
             const u64 j = wfirst + (u64)r * 32u + lane;
             const bool valid = j < nb;
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
             blk = __shfl_sync(kFullMask, bj, 31);
             cnt = __shfl_sync(kFullMask, cj, 31);
             start += __shfl_sync(kFullMask, ci, 31);
-            if (write && valid) {
+            if (valid) {
                 blk_out[j] = bj;
                 if (cj > 0 && sj < units) {  // non-empty block (the reference skips empty ones)
                     is_start[sj] = 1;
@@ -164,13 +164,27 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
         }
     };
     {
-        u64 blk = 0, cnt = 0, start = 0;
-        pass(blk, cnt, start, false);
+        // From zero carries the warp ends at blk = sum of db, cnt = sum of dc, and start = the
+        // sum of its m blocks' counts c_j = dc_0 + .. + dc_j, which is the sum over i of
+        // dc_i * (m - i) (u64, wrapping like the running sums).
         const u64 wbeg = wfirst < nb ? wfirst : nb;
         const u64 nvalid = (nb - wbeg) < 32u * kItems ? nb - wbeg : 32u * kItems;
+        u64 sb = 0, sc = 0, sw = 0;
+        for (int r = 0; r < kItems; ++r) {
+            const u64 i = (u64)r * 32u + lane;
+            if (wfirst + i < nb) {
+                const u64 dc = delta_c(wfirst + i);
+                sb += delta_b(wfirst + i);
+                sc += dc;
+                sw += dc * (nvalid - i);
+            }
+        }
+        sb = warp_sum(sb);
+        sc = warp_sum(sc);
+        sw = warp_sum(sw);
         if (lane == 0) {
-            wsb[w] = blk;
-            wtc[w] = Tri{cnt, nvalid, start};
+            wsb[w] = sb;
+            wtc[w] = Tri{sc, nvalid, sw};
         }
     }
     __syncthreads();
@@ -196,7 +210,7 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
     __syncthreads();
     const Tri pre = TriOp{}(base_c, wtc[w]);
     u64 blk = base_b + wsb[w], cnt = pre.a, start = pre.b;
-    pass(blk, cnt, start, true);
+    pass(blk, cnt, start);
 }
 
 // ---------------------------------------------------------------- units --------------
