@@ -176,14 +176,14 @@ __global__ void __launch_bounds__(kThreads, PAYLOAD ? 3 : 4) sort_pass_kernel(co
         }
     }
     const u64 before = tile == 0 ? 0ull : digit_lookback(status, tile, (u32)tid, tile_count, epoch, err, pre);
-    gbase[tid] = (u64)offsets[tid] + before;
+    gbase[tid] = (u64)offsets[tid] + before - dstart[tid];  // + tile slot p: the output position (u64, wrapping)
     __syncthreads();
 
     const u32 cnt = (u32)min((u64)kTile, n - base);
     for (u32 p = tid; p < cnt; p += kThreads) {
         const u64 key = skeys[p];
         const u32 d = (u32)(key >> shift) & 255u;
-        const u64 o = gbase[d] + (p - dstart[d]);
+        const u64 o = gbase[d] + p;
         if (o >= n) {  // only after an expired look-back wait: flagged, never written
             atomicOr(err, kErrPlacement);
             continue;
