@@ -308,6 +308,18 @@ uint64_t spread3_host(uint32_t v) {
     return r;
 }
 
+// The length shared by every codeword of a code table (len[s] = 0: symbol absent) when it is
+// 1..24 bits, else 0.
+int fixed_code_len(const uint8_t* len, size_t count) {
+    int l = 0;
+    for (size_t s = 0; s < count; ++s) {
+        if (!len[s]) continue;
+        if (!l) l = len[s];
+        else if (len[s] != l) return 0;
+    }
+    return l >= 1 && l <= 24 ? l : 0;
+}
+
 // ---------------------------------------------------------------- sort ------------------
 struct SortBufs {
     unsigned long long* keys[2];
@@ -973,19 +985,36 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         launch_gr_encode(uo.patches, P, grk, at<uint32_t>(c, o_w_gr), 32 * words_for(bits_gr), chan(0),
                          SMALL_FIELD(c, tile_counters[0]), SMALL_FIELD(c, totals[0]), SMALL_FIELD(c, err), side(c, 0));
     }
+    // A code whose codewords all have one length (quads at fine bounds: eight 3-bit codes;
+    // most -rle count streams: two 1-bit codes) places symbol i at bits [i L, (i + 1) L).
+    const int fl_rep = fixed_code_len(c->h_small->codes[0].len, 256);
+    const int fl_quad = fixed_code_len(c->h_small->codes[1].len, 256);
+    const int fl_cnt = (rle && !code_cnt.exp_golomb && sparse_val.empty()) ? fixed_code_len(dense_len.data(), kCountDense) : 0;
     if (!ext && !code_rep.exp_golomb) {
         Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_rep / 8.0, side(c, 1));
-        launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
-                              chan(1), SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err),
-                              side(c, 1));
+        if (fl_rep)
+            launch_fixed_encode_u8(uo.rep_sym, U, c->d_small->codes[0].bits, fl_rep, at<uint32_t>(c, o_w_rep),
+                                   SMALL_FIELD(c, totals[1]), side(c, 1));
+        else
+            launch_huff_encode_u8(uo.rep_sym, U, &c->d_small->codes[0], at<uint32_t>(c, o_w_rep), 32 * words_for(bits_rep),
+                                  chan(1), SMALL_FIELD(c, tile_counters[1]), SMALL_FIELD(c, totals[1]), SMALL_FIELD(c, err),
+                                  side(c, 1));
     }
     if (!direct) {
         Prof pr(c, "encode_huffman", 1, 1.0 * U + bits_quad / 8.0, side(c, 2));
-        launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
-                              32 * words_for(bits_quad), chan(2), SMALL_FIELD(c, tile_counters[2]),
-                              SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), side(c, 2));
+        if (fl_quad)
+            launch_fixed_encode_u8(uo.quad_sym, U, c->d_small->codes[1].bits, fl_quad, at<uint32_t>(c, o_w_quad),
+                                   SMALL_FIELD(c, totals[2]), side(c, 2));
+        else
+            launch_huff_encode_u8(uo.quad_sym, U, &c->d_small->codes[1], at<uint32_t>(c, o_w_quad),
+                                  32 * words_for(bits_quad), chan(2), SMALL_FIELD(c, tile_counters[2]),
+                                  SMALL_FIELD(c, totals[2]), SMALL_FIELD(c, err), side(c, 2));
     }
-    if (rle) {
+    if (rle && fl_cnt) {
+        Prof pr(c, "encode_counts", 1, 4.0 * U + bits_cnt / 8.0, side(c, 3));
+        launch_fixed_encode_i32(at<int32_t>(c, o_counts), U, dbits, fl_cnt, at<uint32_t>(c, o_w_cn),
+                                SMALL_FIELD(c, totals[3]), side(c, 3));
+    } else if (rle) {
         Prof pr(c, "encode_counts", 1, 4.0 * U + bits_cnt / 8.0, side(c, 3));
         launch_count_encode(at<int32_t>(c, o_counts), U, code_cnt.exp_golomb ? code_cnt.eg_k : -1, dbits, dlen, sval,
                             sbits, slen, static_cast<uint32_t>(sparse_val.size()), at<uint32_t>(c, o_w_cn),

@@ -474,6 +474,38 @@ __global__ void __launch_bounds__(kThreads) huff_encode_u8_kernel(const u8* __re
     run.end();
 }
 
+// A prefix code whose codewords all have one length L (1..24 bits): symbol i occupies stream
+// bits [i L, (i + 1) L), so no scan is needed.  Thread g codes symbols [32 g, 32 g + 32), whose
+// 32 L bits fill exactly words [g L, g L + L), MSB-first and stored byte-swapped as MsbRun
+// stores them; whole words, no atomics.  Symbols index code_bits (counts: the dense table).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) fixed_encode_kernel(const T* __restrict__ sym, u64 n,
+                                                                const u32* __restrict__ code_bits, int len,
+                                                                u32* __restrict__ words,
+                                                                unsigned long long* total_bits) {
+    const u64 g = (u64)blockIdx.x * kThreads + threadIdx.x;
+    const u64 total = n * (u64)len;
+    if (g == 0) *total_bits = total;
+    const u64 s0 = g * 32u;
+    if (s0 >= n) return;
+    const u32 mask = (1u << len) - 1u;
+    u64 acc = 0, w = g * (u64)len;
+    u32 nb = 0;
+#pragma unroll 4
+    for (int i = 0; i < 32; ++i) {
+        const u64 idx = s0 + (u64)i;
+        const u32 c = idx < n ? (__ldg(&code_bits[(u32)sym[idx]]) & mask) : 0u;
+        acc = (acc << len) | c;
+        nb += (u32)len;
+        if (nb >= 32u) {
+            nb -= 32u;
+            if (w * 32u < total) words[w] = __byte_perm((u32)(acc >> nb), 0, 0x0123);
+            ++w;
+            acc &= nb ? ((1ull << nb) - 1ull) : 0ull;
+        }
+    }
+}
+
 __device__ __forceinline__ u32 rev_low(u64 v, int k) { return k ? (__brev((u32)v) >> (32 - k)) : 0u; }
 
 __global__ void __launch_bounds__(kThreads) count_encode_kernel(const i32* __restrict__ counts, u64 n, int eg_k,
@@ -594,6 +626,18 @@ void launch_gr_encode(const unsigned long long* vals, uint64_t n, int k, uint32_
     const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
     if (!tiles) return;
     gr_encode_kernel<<<tiles, kThreads, 0, st>>>(vals, n, k, words, cap_bits, lb, tile_counter, total_bits, err);
+}
+void launch_fixed_encode_u8(const uint8_t* sym, uint64_t n, const uint32_t* code_bits, int len, uint32_t* words,
+                            unsigned long long* total_bits, cudaStream_t st) {
+    const u64 threads = (n + 31) / 32;
+    const unsigned blocks = (unsigned)((threads + kThreads - 1) / kThreads);
+    fixed_encode_kernel<u8><<<blocks ? blocks : 1, kThreads, 0, st>>>(sym, n, code_bits, len, words, total_bits);
+}
+void launch_fixed_encode_i32(const int32_t* sym, uint64_t n, const uint32_t* code_bits, int len, uint32_t* words,
+                             unsigned long long* total_bits, cudaStream_t st) {
+    const u64 threads = (n + 31) / 32;
+    const unsigned blocks = (unsigned)((threads + kThreads - 1) / kThreads);
+    fixed_encode_kernel<i32><<<blocks ? blocks : 1, kThreads, 0, st>>>(sym, n, code_bits, len, words, total_bits);
 }
 void launch_huff_encode_u8(const uint8_t* sym, uint64_t n, const ByteCodes* codes, uint32_t* words,
                            uint64_t cap_bits, LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits,

@@ -153,6 +153,12 @@ constexpr int kEncTile = 4096;
 void launch_gr_encode(const unsigned long long* vals, uint64_t n, int k, uint32_t* words, uint64_t cap_bits,
                       LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits, uint32_t* err,
                       cudaStream_t st);
+// A code whose codewords all have one length len (1..24): symbol i at stream bits [i len, (i + 1) len)
+// (code_bits indexed by the symbol; for counts the dense table); *total_bits = n * len.
+void launch_fixed_encode_u8(const uint8_t* sym, uint64_t n, const uint32_t* code_bits, int len, uint32_t* words,
+                            unsigned long long* total_bits, cudaStream_t st);
+void launch_fixed_encode_i32(const int32_t* sym, uint64_t n, const uint32_t* code_bits, int len, uint32_t* words,
+                             unsigned long long* total_bits, cudaStream_t st);
 void launch_huff_encode_u8(const uint8_t* sym, uint64_t n, const ByteCodes* codes, uint32_t* words,
                            uint64_t cap_bits, LookBackState lb, uint32_t* tile_counter, unsigned long long* total_bits,
                            uint32_t* err, cudaStream_t st);
