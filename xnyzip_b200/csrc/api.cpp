@@ -1528,6 +1528,11 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
                             at<unsigned long long>(c, o_xoff), at<unsigned long long>(c, o_rv), SMALL_FIELD(c, err),
                             xs);
     }
+    // A fixed-length -rle count stream sums the point count as it decodes (totals[0], zeroed on
+    // its own stream first).
+    bool counts_summed = false;
+    for (auto& j : jobs)
+        if (rle && j.slot == 3 && j.width == 4 && j.fixed_len && !j.fill) counts_summed = true;
     for (auto& j : jobs) {
         if (j.fill) {
             if (j.width == 1)
@@ -1542,8 +1547,10 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
         if (j.fixed_len) {
             if (j.nsym * static_cast<uint64_t>(j.fixed_len) > j.total_bits)
                 return fail(XNYZ_ERR_BAD_STREAM, "Huffman stream shorter than its symbols");
+            const bool sum = counts_summed && j.slot == 3;
+            if (sum) CUDA_TRY(cudaMemsetAsync(SMALL_FIELD(c, totals), 0, sizeof(unsigned long long) * 8, js));
             launch_decode_fixed(j.words, j.base_bits, j.total_bits, j.table, j.fixed_len, j.nsym, j.width, j.out,
-                                SMALL_FIELD(c, err), js);
+                                SMALL_FIELD(c, err), js, sum ? SMALL_FIELD(c, totals[0]) : nullptr);
             continue;
         }
         // Golomb-Rice tracks k + 2 entry offsets per subsequence (derived in the kernel).
@@ -1563,8 +1570,8 @@ xnyz_status decompress_core(xnyz_ctx* c, const uint8_t* d_cont, uint64_t len, co
     // codeword counts and the error word come back in one copy.  A stream whose parallel
     // decode gave up (rare) is decoded again sequentially and the counts re-summed.
     auto count_total = [&]() -> xnyz_status {
-        TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
-        if (rle && U) {
+        if (!counts_summed) TRY(memset_small(c, offsetof(Small, totals), sizeof(unsigned long long) * 8, 0));
+        if (rle && U && !counts_summed) {
             Prof pr(c, "count_total", 1, 4.0 * U);
             launch_count_total(at<int32_t>(c, o_counts), U, SMALL_FIELD(c, totals[0]), st);
         }

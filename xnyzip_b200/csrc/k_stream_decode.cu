@@ -881,8 +881,10 @@ __global__ void decode_sequential_kernel(Args a) {
 __global__ void __launch_bounds__(256) decode_fixed_kernel(const u32* __restrict__ words, u32 base, u64 nwords,
                                                            int len, const u32* __restrict__ root,
                                                            const u64* __restrict__ symvals, u64 nsym, int width,
-                                                           void* out, bool packed_ok, u32* err) {
+                                                           void* out, bool packed_ok, u32* err,
+                                                           unsigned long long* sum_out) {
     const u64 groups = (nsym + 3) / 4;
+    u64 sum = 0;  // sum_out: the sum of max(symbol, 0) over 32-bit symbols (the -rle point count)
     auto wbe = [&](u64 k) -> u64 { return k < nwords ? (u64)__byte_perm(__ldg(words + k), 0, 0x0123) : 0ull; };
     for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (u64)gridDim.x * blockDim.x) {
         const u64 i0 = 4 * g;
@@ -904,6 +906,7 @@ __global__ void __launch_bounds__(256) decode_fixed_kernel(const u32* __restrict
                 packed |= ((u32)val & 0xffu) << (8 * j);
             } else {
                 reinterpret_cast<u32*>(out)[i0 + j] = (u32)val;
+                sum += (u64)max((i32)(u32)val, 0);
             }
         }
         if (width == 1) {
@@ -915,6 +918,11 @@ __global__ void __launch_bounds__(256) decode_fixed_kernel(const u32* __restrict
             }
         }
         if (bad) atomicOr(err, kErrBadStream);
+    }
+    if (sum_out) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(kFullMask, sum, d);
+        if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(sum_out, sum);
     }
 }
 
@@ -986,7 +994,8 @@ void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, u
 }
 
 void launch_decode_fixed(const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t, int len,
-                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st) {
+                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st,
+                         unsigned long long* sum_out) {
     if (!nsym) return;
     if (len < 1 || len > kMaxRootBits || len != t.root_bits || (out_width != 1 && out_width != 4) ||
         nsym * (uint64_t)len > total_bits) {
@@ -998,7 +1007,8 @@ void launch_decode_fixed(const uint32_t* words, uint64_t base_bits, uint64_t tot
     if (blocks > 148 * 16) blocks = 148 * 16;
     const bool packed_ok = (reinterpret_cast<uintptr_t>(out) & 3u) == 0;
     decode_fixed_kernel<<<(unsigned)blocks, 256, 0, st>>>(words, (u32)base_bits, nwords, len, t.root, t.symvals, nsym,
-                                                          out_width, out, packed_ok, err);
+                                                          out_width, out, packed_ok, err,
+                                                          out_width == 4 ? sum_out : nullptr);
 }
 
 void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,

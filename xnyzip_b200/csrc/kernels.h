@@ -210,9 +210,11 @@ void launch_decode_stream(int kind, const uint32_t* words, uint64_t base_bits, u
                           uint32_t* need_fallback, unsigned long long* total_codewords, cudaStream_t st);
 // One-thread decoder the host runs when a bounded wait of the parallel decoder expired.
 // A Huffman stream whose codewords all have length len (== t.root_bits <= 11): every symbol
-// from its own len bits (out_width 1: u8, 4: u32 values).
+// from its own len bits (out_width 1: u8, 4: u32 values; with out_width 4 and sum_out, *sum_out
+// += the sum of max(value, 0) over the values, as int32).
 void launch_decode_fixed(const uint32_t* words, uint64_t base_bits, uint64_t total_bits, DecodeTable t, int len,
-                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st);
+                         uint64_t nsym, int out_width, void* out, uint32_t* err, cudaStream_t st,
+                         unsigned long long* sum_out = nullptr);
 void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bits, uint64_t total_bits,
                               DecodeTable t, uint64_t nsym, int out_width, void* out,
                               unsigned long long* total_codewords, uint32_t* err, cudaStream_t st);
