@@ -288,8 +288,10 @@ __device__ __forceinline__ u32 quad_step(u32 sq) { return (sq & 8u) ? 0u : ((sq 
 // in shared memory, and folds the warp's counts, quad / block / repos segments (or SFC
 // sums); the block combines the warps, one round of chained scans combines the tiles, and
 // the final pass rebuilds every running value with warp scans from its warp's starting
-// carry.  A tile holding a value of 2^32 or more or a count of 2^16 or more (never in a
-// stream the encoder wrote from a cloud's blocks) re-reads them in the final pass instead.
+// carry.  A tile holding a value of 2^32 or more or a count of 2^16 or more re-reads them
+// in the final pass instead (block mode: never for a stream the encoder wrote, whose repos
+// values are 18-bit codes; direct mode: the tile of a cloud's first SFC code, for example).
+// With every value below 2^26 as well, the rounds' prefix sums run in 32 bits.
 template <bool DIRECT>
 __global__ void __launch_bounds__(kThreads, 6) recover_units_kernel(RecoverArgs a) {
     constexpr int kWarps = kThreads / 32;
