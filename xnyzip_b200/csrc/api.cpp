@@ -617,6 +617,7 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
 
     // ---- 1. bounding box + quantization sweep ----
     HostPhase hp1(c, "c1_stats");
+    int32_t* cells_tmp = nullptr;  // the quantization sweep's cells, when the arena holds them
     {
         PointStats init{};
         for (int a = 0; a < 3; ++a) {
@@ -640,8 +641,11 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         }
         if (adaptive) launch_adaptive_steps(d_xyz, prm.l2_bound, SMALL_FIELD(c, stats), st);
         {
+            // the cells go to the space the units fill later, for the block-mode key kernel
+            const CPlan cp0 = make_cplan(n, want_order, arena_reserved, c->block_mode != XNYZ_BLOCKS_OFF);
+            if (c->arena.cap >= cp0.total) cells_tmp = at<int32_t>(c, cp0.o_patch);  // [o_patch, o_blkunit): 16 n bytes
             Prof pr(c, "quantize_range", 1, 12.0 * n);
-            launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st);
+            launch_quantize_range(d_xyz, n, q, SMALL_FIELD(c, stats), 1, st, cells_tmp);
         }
     }
     CUDA_TRY(cudaGetLastError());
@@ -751,6 +755,9 @@ xnyz_status compress_core(xnyz_ctx* c, const float* d_xyz, uint64_t n, const xny
         else if (direct)
             launch_keys_direct(d_xyz, n, q, SMALL_FIELD(c, stats), dkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
                                passes, c->d_small->sort_hist, st);
+        else if (cells_tmp)
+            launch_keys_cells(cells_tmp, n, bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0], passes,
+                              c->d_small->sort_hist, st);
         else
             launch_keys_block(d_xyz, n, q, SMALL_FIELD(c, stats), bkp, c->d_small->hil_fwd, sb.keys[0], sb.vals[0],
                               passes, c->d_small->sort_hist, st);

@@ -152,7 +152,7 @@ __global__ void adaptive_steps_kernel(const float* __restrict__ xyz, float R, Po
 
 __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* __restrict__ xyz, u64 n,
                                                                   QuantParams q, PointStats* stats,
-                                                                  int with_error_stats) {
+                                                                  int with_error_stats, i32* __restrict__ cells) {
     __shared__ float off[3];
     __shared__ int smax[3][kThreads / 32], smin[3][kThreads / 32];
     __shared__ u32 snf[kThreads / 32], smse[kThreads / 32];
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* _
     u32 nonfinite = 0;
     float emax = 0.0f;
     double esum = 0.0;
-    for_each_point<4>(xyz, n, [&](u64, float x, float y, float z) {
+    for_each_point<4>(xyz, n, [&](u64 i, float x, float y, float z) {
         if (!finite3(x, y, z)) {
             ++nonfinite;
             return;
@@ -177,6 +177,11 @@ __global__ void __launch_bounds__(kThreads) quantize_range_kernel(const float* _
         const float px = __fsub_rn(x, ox), py = __fsub_rn(y, oy), pz = __fsub_rn(z, oz);
         i32 c[3];
         quantize(q, px, py, pz, c[0], c[1], c[2]);
+        if (cells) {  // kept for the key kernel (keys_cells_kernel), which then need not quantize again
+            cells[3 * i] = c[0];
+            cells[3 * i + 1] = c[1];
+            cells[3 * i + 2] = c[2];
+        }
         for (int a = 0; a < 3; ++a) {
             mx[a] = max(mx[a], c[a]);
             mn[a] = min(mn[a], c[a]);
@@ -476,8 +481,8 @@ void launch_adaptive_steps(const float* xyz, float l2, PointStats* stats, cudaSt
     adaptive_steps_kernel<<<1, 32, 0, st>>>(xyz, l2, stats);
 }
 void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
-                           cudaStream_t st) {
-    quantize_range_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, with_error_stats);
+                           cudaStream_t st, int32_t* cells) {
+    quantize_range_kernel<<<grid_for(n), kThreads, 0, st>>>(xyz, n, q, stats, with_error_stats, cells);
 }
 void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, BlockKeyParams kp,
                        const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,

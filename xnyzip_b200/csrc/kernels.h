@@ -100,8 +100,9 @@ struct EncodeTotals {
 void launch_bbox(const float* xyz, uint64_t n, PointStats* stats, cudaStream_t st);
 // AdaptiveQuantizer steps from the bounding box (after launch_bbox) into stats->step.
 void launch_adaptive_steps(const float* xyz, float l2, PointStats* stats, cudaStream_t st);
+// cells (optional, 3 n int32): each finite point's lattice cell, for launch_keys_cells.
 void launch_quantize_range(const float* xyz, uint64_t n, QuantParams q, PointStats* stats, int with_error_stats,
-                           cudaStream_t st);
+                           cudaStream_t st, int32_t* cells = nullptr);
 void launch_keys_block(const float* xyz, uint64_t n, QuantParams q, const PointStats* stats, BlockKeyParams kp,
                        const uint8_t* hilbert_tab, unsigned long long* keys, uint32_t* payload, int passes,
                        uint32_t* hist, cudaStream_t st);
