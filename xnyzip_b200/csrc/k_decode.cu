@@ -1,7 +1,8 @@
 // Decompress-side kernels.
 //
-//   bitunpack      BitPacker<uint64_t>::unpack (encoder/bitpacking_encoder.hpp:53-80)
-//   scan_u64       the prefix sums of block_decompressor.hpp:159-161 (u64, wrapping)
+//   block_streams  BitPacker<uint64_t>::unpack (encoder/bitpacking_encoder.hpp:53-80) of the
+//                  block-id and block-count deltas fused with their prefix sums
+//                  (block_decompressor.hpp:159-161, u64, wrapping) and the block-start marks
 //   (the entropy-coded streams are decoded in k_stream_decode.cu)
 //   recover_units  recover_from_lcp_meta (block_quantizer.hpp:154-207) fused with the PFor
 //                  decode, the direct-mode SFC prefix sum (block_decompressor.hpp:86-102), the
@@ -23,60 +24,6 @@ static_assert(kTile == kScanTile, "tile size");
 __device__ __forceinline__ u64 udiv(u64 x, const U64Div& d) {
     const u64 t = __umul64hi(d.m, x);
     return (t + ((x - t) >> d.sh1)) >> d.sh2;
-}
-
-// ------------------------------------------------------------------ bit unpack ----------
-__global__ void __launch_bounds__(kThreads) bitunpack_kernel(const u32* __restrict__ words, u64 base, u64 n,
-                                                             int width, u64* __restrict__ vals) {
-    const u64 stride = (u64)gridDim.x * kThreads;
-    const u64 mask = width >= 64 ? ~0ull : ((1ull << width) - 1);
-    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride)
-        vals[i] = width ? (peek_lsb64(words, base + i * (u64)width) & mask) : 0ull;
-}
-
-// ------------------------------------------------------------------ scan ----------------
-__global__ void __launch_bounds__(kThreads) scan_u64_kernel(const u64* __restrict__ in, u64* __restrict__ out, u64 n,
-                                                            int exclusive, LookBackState lb, u32* tile_counter,
-                                                            unsigned long long* total, u32* err) {
-    __shared__ u64 sv[kTile];
-    __shared__ u64 scratch[16];
-    __shared__ u32 slot;
-    __shared__ u64 sbase;
-    const u32 tile = claim_tile(tile_counter, &slot);
-    const u64 base = (u64)tile * kTile;
-    const u32 cnt = (u32)min((u64)kTile, n - base);
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = (u32)i * kThreads + threadIdx.x;
-        if (e < cnt) sv[e] = in[base + e];
-    }
-    __syncthreads();
-    const u32 e0 = threadIdx.x * kItems;
-    u64 s = 0;
-    for (int i = 0; i < kItems; ++i)
-        if (e0 + i < cnt) s += sv[e0 + i];
-    u64 tot;
-    const u64 ex = block_exclusive<kThreads>(s, 0ull, AddOp{}, scratch, tot);
-    if (threadIdx.x < 32) {
-        LookBack64 l{lb.flag, lb.agg, lb.inc};
-        const u64 before = warp_lookback_add(l, tile, tot, err);
-        if (threadIdx.x == 0) {
-            sbase = before;
-            if (tile == gridDim.x - 1 && total) *total = before + tot;
-        }
-    }
-    __syncthreads();
-    u64 run = sbase + ex;
-    for (int i = 0; i < kItems; ++i)
-        if (e0 + i < cnt) {
-            const u64 v = sv[e0 + i];
-            sv[e0 + i] = exclusive ? run : run + v;
-            run += v;
-        }
-    __syncthreads();
-    for (int i = 0; i < kItems; ++i) {
-        const u32 e = (u32)i * kThreads + threadIdx.x;
-        if (e < cnt) out[base + e] = sv[e];
-    }
 }
 
 // ------------------------------------------------------------- block streams -----------
@@ -213,28 +160,7 @@ __global__ void __launch_bounds__(kThreads) block_streams_kernel(const u32* __re
     pass(blk, cnt, start);
 }
 
-// ---------------------------------------------------------------- units --------------
-__global__ void __launch_bounds__(kThreads) block_starts_kernel(const u64* __restrict__ start_excl,
-                                                                const u64* __restrict__ blk_cnt_unused, u64 nb,
-                                                                u64 units, u8* __restrict__ is_start,
-                                                                u32* __restrict__ start_block, u32* err) {
-    (void)blk_cnt_unused;
-    const u64 stride = (u64)gridDim.x * kThreads;
-    for (u64 b = (u64)blockIdx.x * kThreads + threadIdx.x; b < nb; b += stride) {
-        const u64 st = start_excl[b];
-        const u64 en = (b + 1 < nb) ? start_excl[b + 1] : units;
-        if (en > st && st < units) {  // non-empty block; empty ones are skipped like the reference
-            is_start[st] = 1;
-            start_block[st] = (u32)b;
-        }
-    }
-}
-
-
 // ---------------------------------------------------------------- helpers --------------
-__global__ void fill_u64_kernel(u64* p, u64 n, u64 v) {
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) p[i] = v;
-}
 __global__ void fill_u32_kernel(u32* p, u64 n, u32 v) {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -588,14 +514,6 @@ inline int grid_cap(u64 n) {
 
 }  // namespace
 
-void launch_bitunpack(const uint32_t* words, uint64_t base_bits, uint64_t n, int width, unsigned long long* vals,
-                      cudaStream_t st) {
-    u64 blocks = (n + kThreads - 1) / kThreads;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    if (!blocks) return;
-    bitunpack_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(words, base_bits, n, width, vals);
-}
-
 void launch_block_streams(const uint32_t* words_blk, uint64_t base_blk, int width_blk, const uint32_t* words_cnt,
                           uint64_t base_cnt, int width_cnt, uint64_t nblocks, uint64_t units,
                           unsigned long long* blk_ids, uint8_t* is_start, uint32_t* start_block, LookBackState lb,
@@ -607,18 +525,6 @@ void launch_block_streams(const uint32_t* words_blk, uint64_t base_blk, int widt
                                                      count_total, err);
 }
 
-void launch_scan_u64(const unsigned long long* in, unsigned long long* out, uint64_t n, int exclusive,
-                     LookBackState lb, uint32_t* tile_counter, unsigned long long* total, uint32_t* err,
-                     cudaStream_t st) {
-    const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
-    if (!tiles) return;
-    scan_u64_kernel<<<tiles, kThreads, 0, st>>>(in, out, n, exclusive, lb, tile_counter, total, err);
-}
-
-
-void launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cudaStream_t st) {
-    if (n) fill_u64_kernel<<<grid_cap(n), kThreads, 0, st>>>(p, n, v);
-}
 void launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st) {
     if (n) fill_u32_kernel<<<grid_cap(n), kThreads, 0, st>>>(p, n, v);
 }
@@ -628,13 +534,6 @@ void launch_fill_u8(uint8_t* p, uint64_t n, uint8_t v, cudaStream_t st) {
 void launch_count_total(const int32_t* counts, uint64_t n, unsigned long long* total, cudaStream_t st) {
     if (n) count_total_kernel<<<grid_cap(n), kThreads, 0, st>>>(counts, n, total);
 }
-void launch_block_starts(const unsigned long long* start_excl, uint64_t nblocks, uint64_t units, uint8_t* is_start,
-                         uint32_t* start_block, uint32_t* err, cudaStream_t st) {
-    if (nblocks)
-        block_starts_kernel<<<grid_cap(nblocks), kThreads, 0, st>>>(start_excl, nullptr, nblocks, units, is_start,
-                                                                    start_block, err);
-}
-
 void launch_recover_units(const RecoverInputs& in, uint64_t units, uint64_t nout, RecoverParams rp,
                           const uint8_t* hilbert_inv_tab, uint32_t* flag, unsigned long long* agg,
                           unsigned long long* inc, uint32_t* tile_counter, float* out, uint32_t* err,

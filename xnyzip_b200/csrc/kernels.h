@@ -172,13 +172,7 @@ void launch_count_encode(const int32_t* counts, uint64_t n, int eg_k, const uint
                          cudaStream_t st);
 
 // --- decompress -------------------------------------------------------------------------
-void launch_bitunpack(const uint32_t* words, uint64_t base_bits, uint64_t n, int width, unsigned long long* vals,
-                      cudaStream_t st);
-// Inclusive (exclusive = 0) or exclusive prefix sums of u64 values (wrapping), in place allowed.
-constexpr int kScanTile = 4096;
-void launch_scan_u64(const unsigned long long* in, unsigned long long* out, uint64_t n, int exclusive,
-                     LookBackState lb, uint32_t* tile_counter, unsigned long long* total, uint32_t* err,
-                     cudaStream_t st);
+constexpr int kScanTile = 4096;  // elements per tile of the decompress-side chained scans
 
 // Parallel decoding of one unindexed prefix-code stream (Huffman, Golomb-Rice, exp-Golomb),
 // implemented in k_stream_decode.cu.
@@ -220,7 +214,6 @@ void launch_decode_sequential(int kind, const uint32_t* words, uint64_t base_bit
                               DecodeTable t, uint64_t nsym, int out_width, void* out,
                               unsigned long long* total_codewords, uint32_t* err, cudaStream_t st);
 void launch_count_total(const int32_t* counts, uint64_t n, unsigned long long* total, cudaStream_t st);
-void launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cudaStream_t st);
 void launch_fill_u8(uint8_t* p, uint64_t n, uint8_t v, cudaStream_t st);
 void launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st);
 
@@ -277,8 +270,6 @@ void launch_block_streams(const uint32_t* words_blk, uint64_t base_blk, int widt
                           uint64_t base_cnt, int width_cnt, uint64_t nblocks, uint64_t units,
                           unsigned long long* blk_ids, uint8_t* is_start, uint32_t* start_block, LookBackState lb,
                           uint32_t* tile_counter, unsigned long long* count_total, uint32_t* err, cudaStream_t st);
-void launch_block_starts(const unsigned long long* start_excl, uint64_t nblocks, uint64_t units, uint8_t* is_start,
-                         uint32_t* start_block, uint32_t* err, cudaStream_t st);
 // flag: [5 * tiles]; agg, inc: [10 * tiles]; tiles = ceil(units / 4096)
 void launch_recover_units(const RecoverInputs& in, uint64_t units, uint64_t nout, RecoverParams rp,
                           const uint8_t* hilbert_inv_tab, uint32_t* flag, unsigned long long* agg,
