@@ -330,34 +330,44 @@ __global__ void __launch_bounds__(kThreads) block_deltas_kernel(const u64* __res
 }
 
 // BitPacker: value b at bit b*width, LSB-first.  A warp packs 32 consecutive values (b0 a
-// multiple of 32), which fill exactly `width` whole words of their own.  For widths 8..32,
-// lane j builds word j from the at most ceil(32 / width) + 1 values it overlaps (shuffles)
-// and stores it; other widths go through the warp's segmented-OR writer.  (Packing 32
-// values per thread into whole words, measured slower: 2.8 -> 4.9 ms per 64M-point step,
-// the per-thread 256-byte reads and width-word writes coalesce worse.)
+// multiple of 32), which fill exactly `width` whole words of their own.  For widths 8..64,
+// lane j builds words j and j + 32 (those below `width`) from the at most ceil(32 / width) + 1
+// values each overlaps (shuffles) and stores them; narrower widths go through the warp's
+// segmented-OR writer.  (Packing 32 values per thread into whole words, measured slower: 2.8
+// -> 4.9 ms per 64M-point step, the per-thread 256-byte reads and width-word writes coalesce
+// worse.)
 __global__ void __launch_bounds__(kThreads) bitpack_kernel(const u64* __restrict__ vals, u64 n, int width,
                                                            u32* words) {
     const u64 stride = (u64)gridDim.x * kThreads;
     const u32 lane = lane_id();
-    if (width >= 8 && width <= 32) {
+    if (width >= 8 && width <= 64) {
         const u32 wu = (u32)width;
         const int K = (int)((32u + wu - 1u) / wu) + 1;
-        const u32 v0 = lane < wu ? (32u * lane) / wu : 0u;  // first value overlapping word `lane`
-        const int p0 = (int)(v0 * wu) - (int)(32u * lane);  // its first bit relative to the word (<= 0)
-        const u64 vmask = (1ull << wu) - 1ull;
+        const int halves = wu > 32u ? 2 : 1;
+        u32 v0[2];
+        int p0[2];
+        for (int h = 0; h < 2; ++h) {
+            const u32 m = lane + 32u * (u32)h;
+            v0[h] = m < wu ? (32u * m) / wu : 0u;                // first value overlapping word m
+            p0[h] = (int)(v0[h] * wu) - (int)(32u * m);         // its first bit relative to the word (<= 0)
+        }
+        const u64 vmask = wu >= 64u ? ~0ull : ((1ull << wu) - 1ull);
         const u64 total = n * (u64)wu;
         for (u64 b0 = (u64)blockIdx.x * kThreads + (threadIdx.x & ~31u); b0 < n; b0 += stride) {
             const u64 b = b0 + lane;
             const u64 x = b < n ? (vals[b] & vmask) : 0ull;
-            u32 word = 0;
-            for (int k = 0; k < K; ++k) {
-                const u32 v = v0 + (u32)k;
-                const u64 xv = __shfl_sync(kFullMask, x, (int)(v & 31u));
-                const int pos = p0 + k * (int)wu;
-                if (lane < wu && v < 32u && pos < 32) word |= pos >= 0 ? (u32)(xv << pos) : (u32)(xv >> (-pos));
+            for (int h = 0; h < halves; ++h) {
+                const u32 m = lane + 32u * (u32)h;
+                u32 word = 0;
+                for (int k = 0; k < K; ++k) {
+                    const u32 v = v0[h] + (u32)k;
+                    const u64 xv = __shfl_sync(kFullMask, x, (int)(v & 31u));
+                    const int pos = p0[h] + k * (int)wu;
+                    if (m < wu && v < 32u && pos < 32) word |= pos >= 0 ? (u32)(xv << pos) : (u32)(xv >> (-pos));
+                }
+                const u64 wi = (b0 >> 5) * (u64)wu + m;
+                if (m < wu && wi * 32u < total) words[wi] = word;
             }
-            const u64 wi = (b0 >> 5) * (u64)wu + lane;
-            if (lane < wu && wi * 32u < total) words[wi] = word;
         }
         return;
     }
