@@ -348,11 +348,33 @@ __device__ bool gr_lockstep_table(const Src& src, u64 B, u64 Bend, int k, u32* t
     u64 gb = act;     // first entry of every group
     u64 alive = act;  // entries not yet recorded
     u32 base = 0, n = 0, exit0 = kOOD, count0 = 0;
+    // The 128 bits from B + base, kept in five stream words that move forward with base (the
+    // groups only advance), instead of two six-word reads per step.
+    u64 wk = (src.base + B) >> 5;
+    u32 wv[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) wv[i] = src.word(wk + i);
     while (__any_sync(kFullMask, act != 0ull)) {
         u64 z0 = 0, z1 = 0;
         if (act) {
-            z0 = ~src.lsb64(B + base);
-            z1 = ~src.lsb64(B + base + 64);
+            const u64 q = src.base + B + base;
+            const u64 kk = q >> 5;
+            if (kk - wk >= 5) {
+                wk = kk;
+#pragma unroll
+                for (int i = 0; i < 5; ++i) wv[i] = src.word(wk + i);
+            } else {
+                while (wk < kk) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) wv[i] = wv[i + 1];
+                    wv[4] = src.word(wk + 5);
+                    ++wk;
+                }
+            }
+            const u32 o = (u32)(q & 31u);
+            const u64 a = (u64)wv[0] | ((u64)wv[1] << 32), b = (u64)wv[2] | ((u64)wv[3] << 32);
+            z0 = ~(o ? (a >> o) | (b << (64u - o)) : a);
+            z1 = ~(o ? (b >> o) | ((u64)wv[4] << (64u - o)) : b);
             ++n;
         }
         // successors, in order; groups landing on the previous group's position merge
